@@ -1,0 +1,189 @@
+/*
+ * netflux_b200.h — C ABI of the B200 implementation of NetFlux's explicit
+ * second-order Euler step.
+ *
+ * Plain C types only (pointers, sizes, ints, doubles); no CUDA or torch types
+ * cross this boundary. Every function returns 0 (NF_OK) on success or an
+ * NF_ERR_* code; the text of the last error of a solver is available from
+ * nf_last_error(), of a failed mesh or solver creation from nf_last_error(NULL).
+ *
+ * Each entry point replaces one piece of the reference's C++ call path
+ * (file:line in andersresell/NetFlux):
+ *
+ *   nf_mesh_from_su2 / nf_mesh_from_arrays
+ *       geometry::PrimalGrid(config) + geometry::FV_Grid(config, primal)
+ *       (PrimalGrid.cpp:140-244, FV_Grid.cpp:21-205)
+ *   nf_create          EulerSolver::EulerSolver (Solver.cpp:135-142)
+ *   nf_set_state / nf_get_state
+ *                      SolverData::get_solution (SolverData.hpp:46-47) — the
+ *                      AoS double[N][5] the reference's Output reads
+ *   nf_calc_timestep   EulerSolver::calc_timestep (Solver.cpp:232-274)
+ *   nf_set_timestep    Config::set_delta_time (Config.hpp:146)
+ *   nf_step            Solver::step (Solver.cpp:34-52): TVD_RK3 (103-133) or
+ *                      explicit_euler (83-101)
+ *   nf_advance         n iterations of Driver::solve's loop body
+ *                      (Driver.cpp:38-47) without host round trips
+ *   nf_get_field       the SolverData accessors get_primvars / _gradient /
+ *                      _limiter / get_flux_balance (SolverData.hpp:52-68)
+ *   nf_destroy         ~Solver
+ *
+ * Threading: a solver handle is bound to the CUDA device that was current
+ * when it was created and to its own stream; it is not re-entrant.
+ */
+#ifndef NETFLUX_B200_H
+#define NETFLUX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define NF_OK 0
+#define NF_ERR_ARG 1          /* invalid argument or size mismatch */
+#define NF_ERR_MESH 2         /* unreadable or invalid mesh */
+#define NF_ERR_CUDA 3         /* a CUDA call failed */
+#define NF_ERR_NONPHYSICAL 4  /* non-finite values or rho <= 0 / p <= 0 */
+#define NF_ERR_DT 5           /* invalid time step (not finite or <= 0) */
+#define NF_ERR_UNSUPPORTED 6  /* option not implemented */
+
+/* ---- enums (same meaning and order as the reference's, Utilities.hpp) ---- */
+#define NF_BC_NO_SLIP_WALL 0  /* BoundaryType::NoSlipWall */
+#define NF_BC_SLIP_WALL 1     /* BoundaryType::SlipWall */
+#define NF_BC_FAR_FIELD 2     /* BoundaryType::FarField */
+
+#define NF_EXPLICIT_EULER 0   /* TimeScheme::ExplicitEuler */
+#define NF_TVD_RK3 1          /* TimeScheme::TVD_RK3 */
+
+#define NF_FIRST_ORDER 0      /* SpatialOrder::First */
+#define NF_SECOND_ORDER 1     /* SpatialOrder::Second */
+
+#define NF_LIMITER_NONE 0     /* Limiter::NONE */
+#define NF_LIMITER_BARTH 1    /* Limiter::Barth */
+
+#define NF_FLUX_RUSANOV 0     /* InviscidFluxScheme::Rusanov */
+
+/* Arithmetic of the step. */
+#define NF_PREC_FP64_REF 0    /* FP64 in the reference's operation order, no FMA
+                                 contraction, true divisions: reproduces the
+                                 reference to the last bit except pow() */
+#define NF_PREC_FP64 1        /* FP64 throughout, FMA and reciprocals allowed */
+#define NF_PREC_MIXED 2       /* FP64 state / RK combine / dt / norms; FP32
+                                 gradient, limiter, reconstruction and flux */
+
+/* nf_get_field selectors */
+#define NF_FIELD_SOLUTION 0   /* U  [N][5] */
+#define NF_FIELD_PRIMVARS 1   /* V of the last evaluated stage [N][5] (interior) */
+#define NF_FIELD_GRADIENT 2   /* grad V [N][15], entry (k,d) at 5*d+k as in the reference */
+#define NF_FIELD_LIMITER 3    /* Barth limiter [N][5] */
+#define NF_FIELD_FLUX_BALANCE 4 /* R of the last stage [N][5] (needs keep_flux_balance) */
+#define NF_FIELD_LOCAL_DT 5   /* per-cell dt [N] (local time stepping) */
+
+typedef struct nf_mesh nf_mesh;
+typedef struct nf_solver nf_solver;
+
+typedef struct {
+  int64_t n_nodes;
+  int64_t n_interior_cells;  /* Config::get_N_INTERIOR_CELLS */
+  int64_t n_ghost_cells;     /* = boundary faces */
+  int64_t n_interior_faces;  /* Config::get_N_INTERIOR_FACES */
+  int64_t n_total_faces;     /* Config::get_N_TOTAL_FACES */
+  int32_t n_patches;
+  int32_t max_faces_per_cell;
+  int64_t n_uncovered_boundary_faces; /* tet faces on the boundary that no
+                                         marker lists; the reference drops them
+                                         (FV_Grid.cpp:79-85) and so does this */
+  int32_t n_cases;           /* concatenated cases (1 unless batched) */
+  int32_t reserved;
+} nf_mesh_info;
+
+/* Build the face-based grid from an SU2 file. patch_names/patch_types give
+ * the boundary type of every marker, like input.yml's "patches:" list; a
+ * marker missing from the list is an error (PrimalGrid.cpp:216-217). Only
+ * tetrahedral volume elements are accepted. */
+nf_mesh* nf_mesh_from_su2(const char* path, int n_patch_types, const char* const* patch_names,
+                          const int* patch_types);
+
+/* The same from arrays: nodes [n_nodes][3]; tets [n_cells][4] node ids in the
+ * order an SU2 file lists them; markers: n_markers names, marker_tris
+ * [sum][3] with marker_offsets[n_markers+1] delimiting each marker. */
+nf_mesh* nf_mesh_from_arrays(int64_t n_nodes, const double* nodes, int64_t n_cells, const int64_t* tets,
+                             int n_markers, const char* const* marker_names, const int* marker_types,
+                             const int64_t* marker_offsets, const int64_t* marker_tris);
+
+/* Concatenate meshes into one batched mesh (cells, faces and patches of case
+ * b follow those of case b-1). Every case keeps its own patches. */
+nf_mesh* nf_mesh_concat(int n, const nf_mesh* const* meshes);
+
+int nf_mesh_get_info(const nf_mesh* m, nf_mesh_info* out);
+/* Patch p: boundary type, first face, number of faces, owning case, name. */
+int nf_mesh_get_patch(const nf_mesh* m, int p, int* type, int64_t* first_face, int64_t* n_faces,
+                      int* case_index, char* name, size_t name_len);
+/* Face-based grid in the reference's order (FV_Grid accessors): face_ij
+ * [F][2] (ghost j >= n_interior_cells), S/ri/rj [F][3], vol and centroid for
+ * all cells incl. ghosts [Nt], [Nt][3], dS [Nc][3]. Any pointer may be NULL. */
+int nf_mesh_export(const nf_mesh* m, uint32_t* face_ij, double* S, double* ri, double* rj, double* vol,
+                   double* centroid, double* dS);
+/* Device cell index of every reference cell (the space-filling-curve
+ * renumbering), [Nc]. */
+int nf_mesh_get_permutation(const nf_mesh* m, int64_t* device_of_ref);
+/* First cell of each case, [n_cases+1]. */
+int nf_mesh_get_case_offsets(const nf_mesh* m, int64_t* cell_offsets);
+void nf_mesh_destroy(nf_mesh* m);
+
+typedef struct {
+  int type;             /* NF_BC_* */
+  double farfield[5];   /* freestream primitives (rho,u,v,w,p) seen by a far-field patch */
+} nf_patch_bc;
+
+typedef struct {
+  int time_scheme;      /* NF_EXPLICIT_EULER / NF_TVD_RK3 */
+  int spatial_order;    /* NF_FIRST_ORDER / NF_SECOND_ORDER */
+  int limiter;          /* NF_LIMITER_NONE / NF_LIMITER_BARTH */
+  int flux_scheme;      /* NF_FLUX_RUSANOV */
+  int precision;        /* NF_PREC_* */
+  int local_time_stepping; /* 0: one global dt (reference); 1: per-cell dt */
+  int dt_from_current_state; /* 0: dt from the primitives of the last
+                                evaluated stage, as the reference does
+                                (Solver.cpp:250); 1: from the current state */
+  int keep_flux_balance;     /* store R of every stage for nf_get_field */
+  double cfl;
+  double t_end;         /* > 0: nf_advance clips dt so time never passes t_end */
+  /* Boundary conditions per patch of the mesh, in patch order. NULL: every
+   * patch uses the mesh's type and the far-field state below. */
+  const nf_patch_bc* patches;
+  int n_patches;
+  double freestream[5]; /* Config::get_primvars_inf (rho,u,v,w,p) */
+  int block_size;       /* 0: tuned default */
+} nf_params;
+
+void nf_params_default(nf_params* p);
+
+nf_solver* nf_create(const nf_mesh* m, const nf_params* params);
+/* U in reference cell order, AoS [n_cells][5]. Setting the state also sets
+ * the primitives the next nf_calc_timestep reads. */
+int nf_set_state(nf_solver* s, const double* U, int64_t n_cells);
+int nf_get_state(nf_solver* s, double* U, int64_t n_cells);
+/* Global dt = min_i CFL*vol_i/sum_d (|u_d|+c) dS_i,d (or the per-cell dt
+ * with local time stepping, then *dt_out is its minimum). */
+int nf_calc_timestep(nf_solver* s, double* dt_out);
+int nf_set_timestep(nf_solver* s, double dt);
+int nf_step(nf_solver* s);
+/* n_steps x (calc_timestep + step) on the device; time (may be NULL) returns
+ * the accumulated time. Uses a CUDA graph after the first call. */
+int nf_advance(nf_solver* s, int64_t n_steps, double* time_out);
+/* Density residual of the first stage of the last step: RMS and max of
+ * R_rho,i / vol_i over all cells (per case: n_cases pairs). */
+int nf_get_residual(nf_solver* s, double* rms_and_max, int n_cases);
+int nf_get_field(nf_solver* s, int which, double* out, int64_t n_values);
+/* Wait for queued work; report a device-side validity failure. */
+int nf_synchronize(nf_solver* s);
+const char* nf_last_error(const nf_solver* s);
+void nf_destroy(nf_solver* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NETFLUX_B200_H */

@@ -1,0 +1,30 @@
+// Host-callable launchers of the device kernels. Each arithmetic form lives
+// in its own translation unit: kernels_ref.cu is compiled with -fmad=false
+// (reference rounding), kernels_fast.cu with contraction on.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+
+namespace nf {
+
+struct Launch {
+  int block;
+  cudaStream_t stream;
+};
+
+// reference-order FP64 (kernels_ref.cu)
+void launch_gradient_ref(const MeshView<double>& m, const StageArgs& a, Launch l);
+void launch_flux_ref(const MeshView<double>& m, const StageArgs& a, Launch l);
+void launch_timestep(const MeshView<double>& m, const DtArgs& a, Launch l);
+void launch_prim_ref(int n, int stride, const double* U, double* V, float* V32, Launch l);
+
+// fast FP64 and mixed FP32/FP64 (kernels_fast.cu)
+void launch_gradient_fast(const MeshView<double>& m, const StageArgs& a, Launch l);
+void launch_flux_fast(const MeshView<double>& m, const StageArgs& a, Launch l);
+void launch_gradient_mixed(const MeshView<float>& m, const StageArgs& a, Launch l);
+void launch_flux_mixed(const MeshView<float>& m, const StageArgs& a, Launch l);
+void launch_prim_fast(int n, int stride, const double* U, double* V, float* V32, Launch l);
+
+}  // namespace nf

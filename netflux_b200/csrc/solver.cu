@@ -1,0 +1,830 @@
+// Solver context and the C ABI declared in include/netflux_b200.h.
+//
+// The context uploads the mesh once (device numbering, see kernels.cuh), owns
+// every device buffer, one stream and the CUDA graphs of the step, and
+// enqueues per step:
+//   [dt reset + timestep kernel]   EulerSolver::calc_timestep
+//   per stage: gradient_limiter, flux_update
+//   [end-of-step kernel]           time += dt (Driver.cpp:47), validity of dt
+// The primitives of successive stage inputs alternate between two buffers, so
+// the buffer that fed the last stage still holds them when the next
+// calc_timestep runs; the reference reads exactly those (Solver.cpp:250).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/netflux_b200.h"
+#include "launch.hpp"
+#include "mesh.hpp"
+
+struct nf_mesh {
+  nf::Mesh m;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+inline void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) ck(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+  }
+  void upload(const std::vector<T>& h, cudaStream_t s) {
+    alloc(h.size());
+    if (n) ck(cudaMemcpyAsync(p, h.data(), n * sizeof(T), cudaMemcpyHostToDevice, s), "cudaMemcpyAsync H2D");
+  }
+  void zero(cudaStream_t s) {
+    if (n) ck(cudaMemsetAsync(p, 0, n * sizeof(T), s), "cudaMemsetAsync");
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DevBuf() { release(); }
+};
+
+__global__ void scal_kernel(double* scal, int op, unsigned* status) {
+  using namespace nf;
+  if (op == 0) {  // reset the dt minimum before the timestep kernel
+    scal[kScalDtMin] = DBL_MAX;
+  } else {  // end of step: time += dt actually used
+    const double dt = stage_dt(scal);
+    if (!(dt > 0.0) || !isfinite(dt)) atomicOr(status, kErrDt);
+    scal[kScalDtUsed] = dt;
+    scal[kScalTime] = scal[kScalTime] + dt;
+  }
+}
+
+// Per-case RMS and max of the per-cell density residual (deterministic: fixed
+// chunking, fixed summation order).
+__global__ void residual_partials_kernel(const double* __restrict__ r, const long long* __restrict__ chunk_begin,
+                                         const long long* __restrict__ chunk_end, double* __restrict__ part) {
+  const int b = blockIdx.x;
+  const long long beg = chunk_begin[b], end = chunk_end[b];
+  double s = 0.0, mx = 0.0;
+  for (long long c = beg + threadIdx.x; c < end; c += blockDim.x) {
+    const double v = r[c];
+    s += v * v;
+    mx = fmax(mx, fabs(v));
+  }
+  __shared__ double ss[256], sm[256];
+  ss[threadIdx.x] = s;
+  sm[threadIdx.x] = mx;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      ss[threadIdx.x] += ss[threadIdx.x + w];
+      sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * b] = ss[0];
+    part[2 * b + 1] = sm[0];
+  }
+}
+
+__global__ void residual_finalize_kernel(const double* __restrict__ part, const int* __restrict__ case_chunk0,
+                                         const long long* __restrict__ case_cells, int n_cases,
+                                         double* __restrict__ out) {
+  const int cs = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cs >= n_cases) return;
+  double s = 0.0, mx = 0.0;
+  for (int b = case_chunk0[cs]; b < case_chunk0[cs + 1]; b++) {
+    s += part[2 * b];
+    mx = fmax(mx, part[2 * b + 1]);
+  }
+  const long long n = case_cells[cs];
+  out[2 * cs] = n > 0 ? sqrt(s / double(n)) : 0.0;
+  out[2 * cs + 1] = mx;
+}
+
+}  // namespace
+
+struct nf_solver {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  nf_params p{};
+  int n = 0, stride = 0, n_faces = 0, n_cases = 1;
+  int block = 256;
+  std::vector<int64_t> dev_of_ref;
+  std::vector<int64_t> case_offsets;
+  std::string err;
+
+  // mesh
+  DevBuf<int> slot, fi, fj;
+  DevBuf<double> S, nhat, area, ri, rj, vol, dS;
+  DevBuf<float> S32, nhat32, area32, ri32, rj32;
+  DevBuf<nf::PatchBC> patches;
+  // state
+  DevBuf<double> U, W, V0, V1, grad, phi, R, dt_local, res_cell, scal, part, res_out;
+  DevBuf<float> V32a, V32b, grad32, phi32;
+  DevBuf<unsigned> status;
+  DevBuf<long long> chunk_begin, chunk_end, case_cells;
+  DevBuf<int> case_chunk0;
+  int n_chunks = 0;
+  double* h_scal = nullptr;  // pinned
+  int vcur = 0;              // V buffer holding the primitives of the current state
+  bool stepped = false;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two steps from vcur = 0 / 1
+
+  double* Vbuf(int i) { return i ? V1.p : V0.p; }
+  float* V32buf(int i) { return i ? V32b.p : V32a.p; }
+  nf::Launch launch() const { return nf::Launch{block, stream}; }
+
+  nf::MeshView<double> view64() const {
+    return nf::MeshView<double>{n, stride, n_faces, slot.p, fi.p, fj.p, S.p, nhat.p, area.p, ri.p, rj.p,
+                                vol.p, dS.p, patches.p};
+  }
+  nf::MeshView<float> view32() const {
+    return nf::MeshView<float>{n, stride, n_faces, slot.p, fi.p, fj.p, S32.p, nhat32.p, area32.p, ri32.p, rj32.p,
+                               vol.p, dS.p, patches.p};
+  }
+
+  void enqueue_dt() {
+    scal_kernel<<<1, 1, 0, stream>>>(scal.p, 0, status.p);
+    nf::DtArgs a;
+    const int vb = p.dt_from_current_state ? vcur : (stepped ? 1 - vcur : vcur);
+    a.V = Vbuf(vb);
+    a.cfl = p.cfl;
+    a.dt_local = p.local_time_stepping ? dt_local.p : nullptr;
+    a.dt_min_bits = reinterpret_cast<unsigned long long*>(scal.p + nf::kScalDtMin);
+    a.status = status.p;
+    nf::launch_timestep(view64(), a, launch());
+  }
+
+  void enqueue_step() {
+    const int n_stages = p.time_scheme == NF_TVD_RK3 ? 3 : 1;
+    for (int s = 0; s < n_stages; s++) {
+      nf::StageArgs a{};
+      a.second_order = p.spatial_order == NF_SECOND_ORDER;
+      a.barth = p.limiter == NF_LIMITER_BARTH;
+      a.scheme = p.time_scheme == NF_TVD_RK3 ? 1 : 0;
+      a.stage = s;
+      a.local_dt = p.local_time_stepping;
+      a.Vin = Vbuf(vcur);
+      a.Vout = Vbuf(1 - vcur);
+      a.grad = grad.p;
+      a.phi = phi.p;
+      a.R = p.keep_flux_balance ? R.p : nullptr;
+      a.res_cell = s == 0 ? res_cell.p : nullptr;
+      a.dt_local = dt_local.p;
+      a.scal = scal.p;
+      a.status = status.p;
+      if (a.scheme == 0) {
+        a.Uin = U.p;
+        a.Uout = U.p;
+      } else if (s == 0) {
+        a.Uin = U.p;
+        a.Uout = W.p;
+      } else if (s == 1) {
+        a.Uin = W.p;
+        a.Un = U.p;
+        a.Uout = W.p;
+      } else {
+        a.Uin = W.p;
+        a.Un = U.p;
+        a.Uout = U.p;
+      }
+      if (p.precision == NF_PREC_MIXED) {
+        a.Vin32 = V32buf(vcur);
+        a.Vout32 = V32buf(1 - vcur);
+        a.grad32 = grad32.p;
+        a.phi32 = phi32.p;
+        if (a.second_order) nf::launch_gradient_mixed(view32(), a, launch());
+        nf::launch_flux_mixed(view32(), a, launch());
+      } else if (p.precision == NF_PREC_FP64) {
+        if (a.second_order) nf::launch_gradient_fast(view64(), a, launch());
+        nf::launch_flux_fast(view64(), a, launch());
+      } else {
+        if (a.second_order) nf::launch_gradient_ref(view64(), a, launch());
+        nf::launch_flux_ref(view64(), a, launch());
+      }
+      vcur = 1 - vcur;
+    }
+    scal_kernel<<<1, 1, 0, stream>>>(scal.p, 1, status.p);
+    stepped = true;
+  }
+
+  // Report a device-side failure as the reference would have (exceptions in
+  // calc_timestep / check_flux_balance_validity become status codes).
+  int check_status() {
+    unsigned st = 0;
+    ck(cudaMemcpyAsync(&st, status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream), "status D2H");
+    ck(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    if (st & nf::kErrNonFinite) {
+      err = "unphysical values detected in the flux_balance field of the Euler solver (non-finite)";
+      return NF_ERR_NONPHYSICAL;
+    }
+    if (st & nf::kErrNonPhysical) {
+      err = "unphysical state: density or pressure <= 0 after an update";
+      return NF_ERR_NONPHYSICAL;
+    }
+    if (st & nf::kErrDt) {
+      err = "Invalid dt calculated";
+      return NF_ERR_DT;
+    }
+    return NF_OK;
+  }
+
+  ~nf_solver() {
+    for (auto& g : graph)
+      if (g) cudaGraphExecDestroy(g);
+    if (h_scal) cudaFreeHost(h_scal);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+template <typename F>
+int guarded(nf_solver* s, F&& fn) {
+  if (!s) return NF_ERR_ARG;
+  try {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != s->device) ck(cudaSetDevice(s->device), "cudaSetDevice");
+    return fn();
+  } catch (const CudaError& e) {
+    s->err = e.what();
+    return NF_ERR_CUDA;
+  } catch (const std::exception& e) {
+    s->err = e.what();
+    return NF_ERR_ARG;
+  }
+}
+
+nf_mesh* wrap_mesh(nf::Mesh&& m) {
+  auto* h = new nf_mesh;
+  h->m = std::move(m);
+  return h;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---------------------------------------------------------------------------
+// mesh
+// ---------------------------------------------------------------------------
+nf_mesh* nf_mesh_from_su2(const char* path, int n_patch_types, const char* const* patch_names,
+                          const int* patch_types) {
+  try {
+    if (!path || n_patch_types < 0 || (n_patch_types && (!patch_names || !patch_types)))
+      throw nf::MeshError("invalid arguments");
+    std::vector<std::string> names;
+    std::vector<int> types;
+    for (int i = 0; i < n_patch_types; i++) {
+      names.emplace_back(patch_names[i]);
+      types.push_back(patch_types[i]);
+    }
+    return wrap_mesh(nf::read_su2(path, names, types));
+  } catch (const std::exception& e) {
+    g_create_error = std::string("Error reading su2 mesh '") + (path ? path : "") + "', " + e.what();
+    return nullptr;
+  }
+}
+
+nf_mesh* nf_mesh_from_arrays(int64_t n_nodes, const double* nodes, int64_t n_cells, const int64_t* tets,
+                             int n_markers, const char* const* marker_names, const int* marker_types,
+                             const int64_t* marker_offsets, const int64_t* marker_tris) {
+  try {
+    if (n_nodes <= 0 || n_cells <= 0 || !nodes || !tets || n_markers < 0 ||
+        (n_markers && (!marker_names || !marker_types || !marker_offsets || !marker_tris)))
+      throw nf::MeshError("invalid arguments");
+    std::vector<double> nd(nodes, nodes + 3 * n_nodes);
+    std::vector<int64_t> tt(tets, tets + 4 * n_cells);
+    std::vector<nf::MarkerInput> mk(static_cast<size_t>(n_markers));
+    for (int i = 0; i < n_markers; i++) {
+      mk[size_t(i)].name = marker_names[i];
+      mk[size_t(i)].type = marker_types[i];
+      const int64_t b = marker_offsets[i], e = marker_offsets[i + 1];
+      if (e < b) throw nf::MeshError("marker offsets must be non-decreasing");
+      mk[size_t(i)].tris.assign(marker_tris + 3 * b, marker_tris + 3 * e);
+    }
+    return wrap_mesh(nf::build_mesh(nd, tt, mk));
+  } catch (const std::exception& e) {
+    g_create_error = std::string("Error creating grid:\n") + e.what();
+    return nullptr;
+  }
+}
+
+nf_mesh* nf_mesh_concat(int n, const nf_mesh* const* meshes) {
+  try {
+    if (n <= 0 || !meshes) throw nf::MeshError("invalid arguments");
+    std::vector<const nf::Mesh*> parts;
+    for (int i = 0; i < n; i++) {
+      if (!meshes[i]) throw nf::MeshError("null mesh");
+      parts.push_back(&meshes[i]->m);
+    }
+    return wrap_mesh(nf::concat_meshes(parts));
+  } catch (const std::exception& e) {
+    g_create_error = std::string("Error concatenating meshes: ") + e.what();
+    return nullptr;
+  }
+}
+
+int nf_mesh_get_info(const nf_mesh* h, nf_mesh_info* out) {
+  if (!h || !out) return NF_ERR_ARG;
+  const nf::Mesh& m = h->m;
+  std::memset(out, 0, sizeof(*out));
+  out->n_nodes = m.n_nodes;
+  out->n_interior_cells = m.n_cells;
+  out->n_ghost_cells = m.n_ghost();
+  out->n_interior_faces = m.n_interior_faces;
+  out->n_total_faces = m.n_faces;
+  out->n_patches = int32_t(m.patches.size());
+  out->max_faces_per_cell = 4;
+  out->n_uncovered_boundary_faces = m.n_uncovered;
+  out->n_cases = m.n_cases();
+  return NF_OK;
+}
+
+int nf_mesh_get_patch(const nf_mesh* h, int p, int* type, int64_t* first_face, int64_t* n_faces, int* case_index,
+                      char* name, size_t name_len) {
+  if (!h || p < 0 || p >= int(h->m.patches.size())) return NF_ERR_ARG;
+  const nf::Patch& P = h->m.patches[size_t(p)];
+  if (type) *type = P.type;
+  if (first_face) *first_face = P.first_face;
+  if (n_faces) *n_faces = P.n_faces;
+  if (case_index) *case_index = P.case_index;
+  if (name && name_len) {
+    std::strncpy(name, P.name.c_str(), name_len - 1);
+    name[name_len - 1] = '\0';
+  }
+  return NF_OK;
+}
+
+int nf_mesh_export(const nf_mesh* h, uint32_t* face_ij, double* S, double* ri, double* rj, double* vol,
+                   double* centroid, double* dS) {
+  if (!h) return NF_ERR_ARG;
+  const nf::Mesh& m = h->m;
+  if (face_ij)
+    for (int64_t f = 0; f < m.n_faces; f++) {
+      face_ij[2 * f] = m.face_i[size_t(f)];
+      face_ij[2 * f + 1] = m.face_j[size_t(f)];
+    }
+  if (S) std::memcpy(S, m.S.data(), m.S.size() * sizeof(double));
+  if (ri) std::memcpy(ri, m.ri.data(), m.ri.size() * sizeof(double));
+  if (rj) std::memcpy(rj, m.rj.data(), m.rj.size() * sizeof(double));
+  if (vol) std::memcpy(vol, m.vol.data(), m.vol.size() * sizeof(double));
+  if (centroid) std::memcpy(centroid, m.centroid.data(), m.centroid.size() * sizeof(double));
+  if (dS) std::memcpy(dS, m.dS.data(), m.dS.size() * sizeof(double));
+  return NF_OK;
+}
+
+int nf_mesh_get_permutation(const nf_mesh* h, int64_t* device_of_ref) {
+  if (!h || !device_of_ref) return NF_ERR_ARG;
+  std::memcpy(device_of_ref, h->m.dev_of_ref.data(), h->m.dev_of_ref.size() * sizeof(int64_t));
+  return NF_OK;
+}
+
+int nf_mesh_get_case_offsets(const nf_mesh* h, int64_t* cell_offsets) {
+  if (!h || !cell_offsets) return NF_ERR_ARG;
+  std::memcpy(cell_offsets, h->m.case_offsets.data(), h->m.case_offsets.size() * sizeof(int64_t));
+  return NF_OK;
+}
+
+void nf_mesh_destroy(nf_mesh* h) { delete h; }
+
+// ---------------------------------------------------------------------------
+// solver
+// ---------------------------------------------------------------------------
+void nf_params_default(nf_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->time_scheme = NF_TVD_RK3;
+  p->spatial_order = NF_SECOND_ORDER;
+  p->limiter = NF_LIMITER_BARTH;
+  p->flux_scheme = NF_FLUX_RUSANOV;
+  p->precision = NF_PREC_FP64;
+  p->cfl = 0.8;
+  p->freestream[0] = 1.225;   // standard air (Utilities.hpp:100-107)
+  p->freestream[4] = 101325.0;
+}
+
+nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
+  if (!h || !params) {
+    g_create_error = "nf_create: null mesh or params";
+    return nullptr;
+  }
+  auto s = std::make_unique<nf_solver>();
+  try {
+    const nf::Mesh& m = h->m;
+    const nf_params& p = *params;
+    if (p.time_scheme != NF_EXPLICIT_EULER && p.time_scheme != NF_TVD_RK3) throw std::runtime_error("bad time_scheme");
+    if (p.spatial_order != NF_FIRST_ORDER && p.spatial_order != NF_SECOND_ORDER)
+      throw std::runtime_error("bad spatial_order");
+    if (p.limiter != NF_LIMITER_NONE && p.limiter != NF_LIMITER_BARTH) throw std::runtime_error("bad limiter");
+    if (p.flux_scheme != NF_FLUX_RUSANOV)
+      throw std::runtime_error("only the Rusanov flux is implemented (the reference's HLLC is a stub)");
+    if (p.precision < NF_PREC_FP64_REF || p.precision > NF_PREC_MIXED) throw std::runtime_error("bad precision");
+    if (p.patches && p.n_patches != int(m.patches.size()))
+      throw std::runtime_error("params.n_patches does not match the mesh's patch count");
+    s->p = p;
+    s->p.patches = nullptr;  // copied below
+    s->block = p.block_size > 0 ? p.block_size : 256;
+    if (s->block % 32 || s->block > 256) throw std::runtime_error("block_size must be a multiple of 32, <= 256");
+    ck(cudaGetDevice(&s->device), "cudaGetDevice");
+    ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    cudaStream_t st = s->stream;
+
+    const int64_t N = m.n_cells, F = m.n_faces;
+    if (N >= (int64_t(1) << 30) || F >= (int64_t(1) << 30)) throw std::runtime_error("mesh too large for one solver");
+    s->n = int(N);
+    s->stride = int((N + 63) / 64 * 64);
+    s->n_faces = int(F);
+    s->dev_of_ref = m.dev_of_ref;
+    s->case_offsets = m.case_offsets;
+    s->n_cases = m.n_cases();
+    const int stride = s->stride;
+
+    // device face order: by the first device cell that touches the face
+    std::vector<int64_t> key(static_cast<size_t>(F));
+    for (int64_t f = 0; f < F; f++) {
+      const int64_t di = m.dev_of_ref[m.face_i[size_t(f)]];
+      const bool interior = m.face_j[size_t(f)] < uint32_t(N);
+      key[size_t(f)] = interior ? std::min(di, m.dev_of_ref[m.face_j[size_t(f)]]) : di;
+    }
+    std::vector<int64_t> dev_face_order(static_cast<size_t>(F));
+    std::iota(dev_face_order.begin(), dev_face_order.end(), 0);
+    std::stable_sort(dev_face_order.begin(), dev_face_order.end(),
+                     [&](int64_t a, int64_t b) { return key[size_t(a)] < key[size_t(b)]; });
+    std::vector<int64_t> fdev(static_cast<size_t>(F));
+    for (int64_t k = 0; k < F; k++) fdev[size_t(dev_face_order[size_t(k)])] = k;
+
+    std::vector<int> h_fi(static_cast<size_t>(F)), h_fj(static_cast<size_t>(F));
+    std::vector<double> h_S(size_t(3 * F)), h_n(size_t(3 * F)), h_a(static_cast<size_t>(F)), h_ri(size_t(3 * F)),
+        h_rj(size_t(3 * F));
+    for (int64_t f = 0; f < F; f++) {
+      const int64_t d = fdev[size_t(f)];
+      h_fi[size_t(d)] = int(m.dev_of_ref[m.face_i[size_t(f)]]);
+      const uint32_t j = m.face_j[size_t(f)];
+      h_fj[size_t(d)] = j < uint32_t(N) ? int(m.dev_of_ref[j]) : -(1 + m.face_patch[size_t(f)]);
+      h_a[size_t(d)] = m.area[size_t(f)];
+      for (int c = 0; c < 3; c++) {
+        h_S[size_t(c * F + d)] = m.S[size_t(3 * f + c)];
+        h_n[size_t(c * F + d)] = m.nhat[size_t(3 * f + c)];
+        h_ri[size_t(c * F + d)] = m.ri[size_t(3 * f + c)];
+        h_rj[size_t(c * F + d)] = m.rj[size_t(3 * f + c)];
+      }
+    }
+    // slots in reference face order
+    std::vector<int> h_slot(size_t(4) * stride, -1);
+    std::vector<int> fill(size_t(stride), 0);
+    auto add_slot = [&](int64_t cell_dev, int value) {
+      int& k = fill[size_t(cell_dev)];
+      if (k >= 4) throw std::runtime_error("a cell has more than 4 faces (only tetrahedra are supported)");
+      h_slot[size_t(k) * stride + size_t(cell_dev)] = value;
+      k++;
+    };
+    for (int64_t f = 0; f < F; f++) {
+      const int fd = int(fdev[size_t(f)]);
+      add_slot(m.dev_of_ref[m.face_i[size_t(f)]], fd << 1);
+      const uint32_t j = m.face_j[size_t(f)];
+      if (j < uint32_t(N)) add_slot(m.dev_of_ref[j], (fd << 1) | 1);
+    }
+    std::vector<double> h_vol(size_t(stride), 1.0), h_dS(size_t(3) * stride, 0.0);
+    for (int64_t c = 0; c < N; c++) {
+      const int64_t d = m.dev_of_ref[size_t(c)];
+      h_vol[size_t(d)] = m.vol[size_t(c)];
+      for (int k = 0; k < 3; k++) h_dS[size_t(k) * stride + size_t(d)] = m.dS[size_t(3 * c + k)];
+    }
+    // boundary conditions per patch
+    std::vector<nf::PatchBC> h_pb(m.patches.size());
+    for (size_t q = 0; q < m.patches.size(); q++) {
+      nf::PatchBC& b = h_pb[q];
+      b.type = params->patches ? params->patches[q].type : m.patches[q].type;
+      b.case_index = m.patches[q].case_index;
+      const double* fs = params->patches ? params->patches[q].farfield : p.freestream;
+      for (int k = 0; k < 5; k++) b.fs[k] = fs[k];
+      // BC_FarField::BC_FarField (Numerics.cpp:76-84)
+      b.c_fs = std::sqrt(nf::Gas<double>::gamma * fs[4] / fs[0]);
+      b.s_fs = fs[4] * std::pow(fs[0], -nf::Gas<double>::gamma);
+      if (b.type < 0 || b.type > 2) throw std::runtime_error("bad boundary type");
+    }
+
+    s->fi.upload(h_fi, st);
+    s->fj.upload(h_fj, st);
+    s->slot.upload(h_slot, st);
+    s->S.upload(h_S, st);
+    s->nhat.upload(h_n, st);
+    s->area.upload(h_a, st);
+    s->ri.upload(h_ri, st);
+    s->rj.upload(h_rj, st);
+    s->vol.upload(h_vol, st);
+    s->dS.upload(h_dS, st);
+    s->patches.upload(h_pb, st);
+    if (p.precision == NF_PREC_MIXED) {
+      auto tof = [](const std::vector<double>& v) {
+        std::vector<float> o(v.size());
+        for (size_t i = 0; i < v.size(); i++) o[i] = float(v[i]);
+        return o;
+      };
+      s->S32.upload(tof(h_S), st);
+      s->nhat32.upload(tof(h_n), st);
+      s->area32.upload(tof(h_a), st);
+      s->ri32.upload(tof(h_ri), st);
+      s->rj32.upload(tof(h_rj), st);
+      s->V32a.alloc(size_t(5) * stride);
+      s->V32b.alloc(size_t(5) * stride);
+      s->grad32.alloc(size_t(15) * stride);
+      s->phi32.alloc(size_t(5) * stride);
+      s->V32a.zero(st);
+      s->V32b.zero(st);
+      s->grad32.zero(st);
+      s->phi32.zero(st);
+    }
+    s->U.alloc(size_t(5) * stride);
+    s->W.alloc(size_t(5) * stride);
+    s->V0.alloc(size_t(5) * stride);
+    s->V1.alloc(size_t(5) * stride);
+    s->grad.alloc(size_t(15) * stride);
+    s->phi.alloc(size_t(5) * stride);
+    if (p.keep_flux_balance) {
+      s->R.alloc(size_t(5) * stride);
+      s->R.zero(st);
+    }
+    s->dt_local.alloc(static_cast<size_t>(stride));
+    s->res_cell.alloc(static_cast<size_t>(stride));
+    s->scal.alloc(nf::kScalCount);
+    s->status.alloc(1);
+    for (auto* b : {&s->U, &s->W, &s->V0, &s->V1, &s->grad, &s->phi, &s->dt_local, &s->res_cell, &s->scal})
+      b->zero(st);
+    s->status.zero(st);
+    // residual chunks: fixed-size pieces of each case's cell range
+    std::vector<long long> cb, ce, cc;
+    std::vector<int> c0{0};
+    const long long chunk = 16384;
+    for (int cs = 0; cs < s->n_cases; cs++) {
+      const long long b0 = m.case_offsets[size_t(cs)], e0 = m.case_offsets[size_t(cs + 1)];
+      for (long long b = b0; b < e0; b += chunk) {
+        cb.push_back(b);
+        ce.push_back(std::min(e0, b + chunk));
+      }
+      if (e0 == b0) {
+        cb.push_back(b0);
+        ce.push_back(b0);
+      }
+      c0.push_back(int(cb.size()));
+      cc.push_back(e0 - b0);
+    }
+    s->n_chunks = int(cb.size());
+    s->chunk_begin.upload(cb, st);
+    s->chunk_end.upload(ce, st);
+    s->case_cells.upload(cc, st);
+    s->case_chunk0.upload(c0, st);
+    s->part.alloc(size_t(2) * s->n_chunks);
+    s->res_out.alloc(size_t(2) * s->n_cases);
+    ck(cudaMallocHost(&s->h_scal, nf::kScalCount * sizeof(double)), "cudaMallocHost");
+    std::fill(s->h_scal, s->h_scal + nf::kScalCount, 0.0);
+    s->h_scal[nf::kScalTEnd] = p.t_end;
+    ck(cudaMemcpyAsync(s->scal.p, s->h_scal, nf::kScalCount * sizeof(double), cudaMemcpyHostToDevice, st),
+       "scal H2D");
+    ck(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    ck(cudaGetLastError(), "nf_create");
+  } catch (const std::exception& e) {
+    g_create_error = std::string("nf_create: ") + e.what();
+    return nullptr;
+  }
+  return s.release();
+}
+
+int nf_set_state(nf_solver* s, const double* U, int64_t n_cells) {
+  return guarded(s, [&]() -> int {
+    if (!U || n_cells != s->n) {
+      s->err = "nf_set_state: state size does not match the mesh";
+      return NF_ERR_ARG;
+    }
+    const int st = s->stride;
+    std::vector<double> h(size_t(5) * st, 0.0);
+    for (int64_t c = 0; c < n_cells; c++) {
+      const int64_t d = s->dev_of_ref[size_t(c)];
+      for (int k = 0; k < 5; k++) h[size_t(k) * st + size_t(d)] = U[5 * c + k];
+    }
+    ck(cudaMemcpyAsync(s->U.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream), "U H2D");
+    // primitives of the initial state in both buffers (the first
+    // calc_timestep reads them, like the harness-initialised reference)
+    for (int b = 0; b < 2; b++) {
+      if (s->p.precision == NF_PREC_FP64_REF)
+        nf::launch_prim_ref(s->n, st, s->U.p, s->Vbuf(b), s->p.precision == NF_PREC_MIXED ? s->V32buf(b) : nullptr,
+                            s->launch());
+      else
+        nf::launch_prim_fast(s->n, st, s->U.p, s->Vbuf(b),
+                             s->p.precision == NF_PREC_MIXED ? s->V32buf(b) : nullptr, s->launch());
+    }
+    s->vcur = 0;
+    s->stepped = false;
+    ck(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream), "status reset");
+    ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
+    ck(cudaGetLastError(), "nf_set_state");
+    return NF_OK;
+  });
+}
+
+int nf_get_state(nf_solver* s, double* U, int64_t n_cells) {
+  return guarded(s, [&]() -> int {
+    if (!U || n_cells != s->n) {
+      s->err = "nf_get_state: state size does not match the mesh";
+      return NF_ERR_ARG;
+    }
+    const int st = s->stride;
+    std::vector<double> h(size_t(5) * st);
+    ck(cudaMemcpyAsync(h.data(), s->U.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "U D2H");
+    ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
+    for (int64_t c = 0; c < n_cells; c++) {
+      const int64_t d = s->dev_of_ref[size_t(c)];
+      for (int k = 0; k < 5; k++) U[5 * c + k] = h[size_t(k) * st + size_t(d)];
+    }
+    return s->check_status();
+  });
+}
+
+int nf_calc_timestep(nf_solver* s, double* dt_out) {
+  return guarded(s, [&]() -> int {
+    s->enqueue_dt();
+    ck(cudaGetLastError(), "timestep launch");
+    ck(cudaMemcpyAsync(s->h_scal, s->scal.p, nf::kScalCount * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
+       "scal D2H");
+    int rc = s->check_status();
+    const double dt = s->h_scal[nf::kScalDtMin];
+    if (dt_out) *dt_out = dt;
+    if (rc == NF_OK && !(std::isfinite(dt) && dt > 0.0)) rc = NF_ERR_DT;
+    if (rc == NF_ERR_DT) {
+      char buf[96];
+      std::snprintf(buf, sizeof(buf), "Invalid dt calculated (dt = %f)", dt);
+      s->err = buf;
+    }
+    return rc;
+  });
+}
+
+int nf_set_timestep(nf_solver* s, double dt) {
+  return guarded(s, [&]() -> int {
+    if (!(dt > 0.0) || !std::isfinite(dt)) {
+      s->err = "nf_set_timestep: dt must be positive and finite";
+      return NF_ERR_ARG;
+    }
+    s->h_scal[nf::kScalCount - 1] = dt;
+    ck(cudaMemcpyAsync(s->scal.p + nf::kScalDtMin, s->h_scal + nf::kScalCount - 1, sizeof(double),
+                       cudaMemcpyHostToDevice, s->stream),
+       "dt H2D");
+    ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
+    return NF_OK;
+  });
+}
+
+int nf_step(nf_solver* s) {
+  return guarded(s, [&]() -> int {
+    s->enqueue_step();
+    ck(cudaGetLastError(), "step launch");
+    return NF_OK;
+  });
+}
+
+int nf_advance(nf_solver* s, int64_t n_steps, double* time_out) {
+  return guarded(s, [&]() -> int {
+    if (n_steps < 0) return NF_ERR_ARG;
+    int64_t left = n_steps;
+    if (left >= 2 && s->stepped) {
+      const int v0 = s->vcur;
+      if (!s->graph[v0]) {
+        // capture two steps: the V buffers return to their roles afterwards
+        cudaGraph_t g = nullptr;
+        ck(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        for (int k = 0; k < 2; k++) {
+          s->enqueue_dt();
+          s->enqueue_step();
+        }
+        ck(cudaStreamEndCapture(s->stream, &g), "end capture");
+        ck(cudaGraphInstantiate(&s->graph[v0], g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
+        s->vcur = v0;
+      }
+      while (left >= 2) {
+        ck(cudaGraphLaunch(s->graph[v0], s->stream), "graph launch");
+        left -= 2;
+      }
+    }
+    while (left > 0) {
+      s->enqueue_dt();
+      s->enqueue_step();
+      left--;
+    }
+    ck(cudaGetLastError(), "advance launch");
+    int rc = s->check_status();
+    if (time_out) {
+      ck(cudaMemcpy(s->h_scal, s->scal.p, nf::kScalCount * sizeof(double), cudaMemcpyDeviceToHost), "scal D2H");
+      *time_out = s->h_scal[nf::kScalTime];
+    }
+    return rc;
+  });
+}
+
+int nf_get_residual(nf_solver* s, double* out, int n_cases) {
+  return guarded(s, [&]() -> int {
+    if (!out || n_cases != s->n_cases) {
+      s->err = "nf_get_residual: n_cases does not match the mesh";
+      return NF_ERR_ARG;
+    }
+    residual_partials_kernel<<<s->n_chunks, 256, 0, s->stream>>>(s->res_cell.p, s->chunk_begin.p, s->chunk_end.p,
+                                                                 s->part.p);
+    residual_finalize_kernel<<<(s->n_cases + 127) / 128, 128, 0, s->stream>>>(s->part.p, s->case_chunk0.p,
+                                                                            s->case_cells.p, s->n_cases,
+                                                                            s->res_out.p);
+    ck(cudaGetLastError(), "residual launch");
+    std::vector<double> h(size_t(2) * s->n_cases);
+    ck(cudaMemcpyAsync(h.data(), s->res_out.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
+       "residual D2H");
+    ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
+    std::copy(h.begin(), h.end(), out);
+    return NF_OK;
+  });
+}
+
+int nf_get_field(nf_solver* s, int which, double* out, int64_t n_values) {
+  return guarded(s, [&]() -> int {
+    const int st = s->stride;
+    const double* src = nullptr;
+    int comps = 5;
+    switch (which) {
+      case NF_FIELD_SOLUTION: src = s->U.p; break;
+      case NF_FIELD_PRIMVARS: src = s->Vbuf(s->stepped ? 1 - s->vcur : s->vcur); break;
+      case NF_FIELD_GRADIENT: src = s->grad.p; comps = 15; break;
+      case NF_FIELD_LIMITER: src = s->phi.p; break;
+      case NF_FIELD_FLUX_BALANCE: src = s->R.p; break;
+      case NF_FIELD_LOCAL_DT: src = s->dt_local.p; comps = 1; break;
+      default: s->err = "nf_get_field: unknown field"; return NF_ERR_ARG;
+    }
+    if (!src) {
+      s->err = "nf_get_field: field not kept (set keep_flux_balance)";
+      return NF_ERR_ARG;
+    }
+    if (!out || n_values != int64_t(comps) * s->n) {
+      s->err = "nf_get_field: output size does not match";
+      return NF_ERR_ARG;
+    }
+    std::vector<double> h(size_t(comps) * st);
+    if (s->p.precision == NF_PREC_MIXED && (which == NF_FIELD_GRADIENT || which == NF_FIELD_LIMITER)) {
+      std::vector<float> hf(size_t(comps) * st);
+      const float* src32 = which == NF_FIELD_GRADIENT ? s->grad32.p : s->phi32.p;
+      ck(cudaMemcpyAsync(hf.data(), src32, hf.size() * sizeof(float), cudaMemcpyDeviceToHost, s->stream), "D2H");
+      ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
+      for (size_t i = 0; i < hf.size(); i++) h[i] = hf[i];
+    } else {
+      ck(cudaMemcpyAsync(h.data(), src, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "D2H");
+      ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
+    }
+    for (int64_t c = 0; c < s->n; c++) {
+      const int64_t d = s->dev_of_ref[size_t(c)];
+      if (which == NF_FIELD_GRADIENT) {
+        // reference layout: Eigen column-major 5x3, entry (k, dim) at 5*dim + k
+        for (int k = 0; k < 5; k++)
+          for (int dm = 0; dm < 3; dm++) out[15 * c + 5 * dm + k] = h[size_t(k * 3 + dm) * st + size_t(d)];
+      } else {
+        for (int k = 0; k < comps; k++) out[comps * c + k] = h[size_t(k) * st + size_t(d)];
+      }
+    }
+    return NF_OK;
+  });
+}
+
+int nf_synchronize(nf_solver* s) {
+  return guarded(s, [&]() -> int { return s->check_status(); });
+}
+
+const char* nf_last_error(const nf_solver* s) { return s ? s->err.c_str() : g_create_error.c_str(); }
+
+void nf_destroy(nf_solver* s) {
+  if (!s) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int own = s->device;
+  if (dev != own) cudaSetDevice(own);
+  cudaStreamSynchronize(s->stream);
+  delete s;
+  if (dev != own) cudaSetDevice(dev);
+}
+
+}  // extern "C"
