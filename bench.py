@@ -1,0 +1,363 @@
+"""Benchmark of the explicit second-order Euler step (TVD-RK3) on B200.
+
+Workload (default): the steady bump channel, [0,3]x[0,1]^2 with a
+0.1*sin^2 bump, 128x64x64 hexes x 6 = 3,145,728 tets, Mach 0.5 free stream,
+local time stepping at CFL 0.8, FP64. One bench step = one TVD-RK3 step
+(3 cell-stages per cell). Synthetic mesh generated in-process; every working
+array is far larger than the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--case bump|cube|sod] [--precision fp64|mixed|fp64_ref]
+
+Prints one JSON line on rank 0. ``value`` is Mcell-RK-stages/s with the state
+resident in HBM (CUDA events on the solver's stream, max over ranks);
+``e2e`` is the same metric through the public API with the state copied
+host->device and back every step; ``roofline`` is the dominant kernel's
+algorithmic HBM bytes per launch over its event-timed duration against the
+measured copy bandwidth; ``cpu_baseline`` is the NetFlux reference compiled
+from its sources, timed on this host's cores on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-RK-stages/s"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--case", default="bump", choices=["bump", "cube", "sod"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "fp64_ref"])
+    ap.add_argument("--scale", type=int, default=1, help="divide the hex counts (quick runs)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--block", type=int, default=0)
+    return ap.parse_args()
+
+
+def case_mesh(name: str, scale: int):
+    from netflux_b200 import meshgen as mg
+    if name == "bump":
+        m = mg.bump_mesh(128 // scale, 64 // scale, 64 // scale, h=0.1)
+        fs = mg.bump_freestream(0.5)
+        return m, fs, mg.uniform_state(m.n_cells, fs), True, "bump channel 128x64x64 hexes, 6 tets each"
+    if name == "cube":
+        m = mg.cube_mesh(20 // scale, jitter=0.1, seed=1234)
+        fs = (1.0, 0.5, 0.0, 0.0, 1.0 / 1.4)
+        return m, fs, mg.cube_initial_state(m), False, "unit cube 20^3 hexes, 6 tets each, Gaussian density bump"
+    m = mg.sod_mesh(400 // scale, 8, 8, jitter=0.05, seed=4321)
+    return m, mg.SOD_LEFT, mg.sod_initial_state(m), False, "Sod tube 400x8x8 hexes, 6 tets each"
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+                for n, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.remove(self.path)
+            except Exception:
+                pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, precision: str):
+    """Compulsory HBM bytes per launch of each kernel (every datum once).
+
+    flux_update, per cell: V, grad, phi of the cell (40+120+40), U of the stage
+    input (40), U^n (40, stages 2 and 3: 2/3 on average), vol (8), 4 slots (16),
+    writes U and V (80); per face: owner/neighbour ids (8), unit normal and
+    area (32), both centroid-to-face vectors (48).
+    gradient_limiter, per cell: V (40), vol (8), slots (16), writes grad and
+    phi (160); per face: ids (8), S (24), both r vectors (48), and the unit
+    normal of boundary faces (24).
+    """
+    r = 4 if precision == "mixed" else 8
+    vcell = 5 * r + 15 * r + 5 * r
+    flux = n_cells * (vcell + 40 + 40 * 2 / 3 + 8 + 16 + 80 + (20 if precision == "mixed" else 0)) \
+        + n_faces * (8 + 4 * r + 6 * r)
+    grad = n_cells * (5 * r + 8 + 16 + 20 * r) + n_faces * (8 + 3 * r + 6 * r) + n_boundary * 3 * r
+    return {"flux": flux, "gradient": grad}
+
+
+def model_bytes_per_cell_stage(n_cells: int, n_faces: int) -> float:
+    """The per-cell-stage byte model of the step's compulsory traffic (FP64):
+    N_c*[3*(40 U read + 40 U write + 8 vol + 240 limited-gradient write+read)
+    + 2*40 U^n read + 24 dS] + N_f*3*80, divided by 3*N_c."""
+    step = n_cells * (3 * (40 + 40 + 8 + 240) + 2 * 40 + 24) + n_faces * 3 * 80
+    return step / (3.0 * n_cells)
+
+
+def cpu_reference_baseline(n_steps: int = 3, scale_hex=(64, 32, 32), procs: int = 0):
+    """Time the compiled reference on a bounded sample of the bump workload."""
+    from netflux_b200 import meshgen as mg
+    from oracle import pyoracle as po  # CPU baseline leg only
+    variant = "nf_ref_nodump"
+    if not po.reference_available(variant):
+        return None
+    nx, ny, nz = scale_hex
+    m = mg.bump_mesh(nx, ny, nz, h=0.1)
+    fs = mg.bump_freestream(0.5)
+    nproc = procs or (os.cpu_count() or 1)
+    with tempfile.TemporaryDirectory() as tmp:
+        case = os.path.join(tmp, "case")
+        mg.write_case(case, m, fs, U0=mg.uniform_state(m.n_cells, fs))
+        exe = os.path.join(po.REF_DIR, variant)
+
+        def run_many(k):
+            outs, ps = [], []
+            for i in range(k):
+                od = os.path.join(tmp, f"o{i}")
+                os.makedirs(od, exist_ok=True)
+                outs.append(od)
+                ps.append(subprocess.Popen([exe, case, od, "--steps", str(n_steps), "--quiet"], cwd=tmp,
+                                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
+            for p in ps:
+                p.wait()
+            secs = []
+            for od in outs:
+                for line in open(os.path.join(od, "meta.txt")):
+                    if line.startswith("seconds"):
+                        secs.append(float(line.split()[1]))
+            return secs
+
+        one = run_many(1)[0]
+        many = run_many(nproc) if nproc > 1 else [one]
+    cs = m.n_cells * 3 * n_steps
+    return {
+        "single_core": cs / one / 1e6,
+        "all_cores": cs * len(many) / max(many) / 1e6,
+        "cores": nproc,
+        "sample": f"bump channel {nx}x{ny}x{nz} hexes ({m.n_cells} tets), {n_steps} TVD-RK3 steps per process, "
+                  f"reference compiled from its sources (debug dump linked out), {nproc} independent "
+                  f"single-threaded processes",
+    }
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import pyoracle as po  # reference arm: the reference's own CPU code
+    if not po.reference_available("nf_ref_nodump"):
+        print(json.dumps({"impl": "reference", "unavailable": "reference build (oracle/_ref) missing"}))
+        return
+    nproc = os.cpu_count() or 1
+    res = cpu_reference_baseline(n_steps=max(1, args.steps), procs=nproc)
+    val = res["all_cores"]
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(val, 3), "unit": "Mcell-stages/s",
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "bump channel, TVD-RK3 FP64 (sample of the 3.1M-tet case)",
+                   "sample": res["sample"]},
+        "cpu_baseline": {"value": round(val, 3), "unit": "Mcell-stages/s", "cores": res["cores"],
+                         "kind": "reference", "sample": res["sample"],
+                         "single_core": round(res["single_core"], 4)},
+        "e2e": {"value": round(val, 3), "unit": "Mcell-stages/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from netflux_b200 import _lib as L
+    from netflux_b200 import solver as S
+
+    m, fs, U0, lts, desc = case_mesh(args.case, args.scale)
+    t0 = time.perf_counter()
+    mesh = S.Mesh.from_tet_mesh(m)
+    t_mesh = time.perf_counter() - t0
+    cfg = S.Config(precision=args.precision, CFL=0.8, local_time_stepping=lts, density_fs=fs[0],
+                   velocity_fs=list(fs[1:4]), pressure_fs=fs[4])
+    solver = S.EulerSolver(cfg, mesh, U0=U0, block_size=args.block)
+    lib = L.load()
+    N = mesh.n_cells
+
+    # warm-up (also builds the CUDA graph of the step)
+    ms = C.c_double()
+    solver.advance(max(args.warmup, 3))
+    kms = (C.c_double * L.NF_KERNEL_COUNT)()
+    kl = (C.c_int64 * L.NF_KERNEL_COUNT)()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        rc = lib.nf_time_steps(solver._h, args.steps, 0, C.byref(ms), kms, kl)
+    if rc != 0:
+        raise RuntimeError(L.last_error(solver._h))
+    torch.cuda.synchronize()
+    dev_ms = ms.value
+    if dist:
+        t = torch.tensor([dev_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t.item())
+        dist.barrier()
+    value = world * N * 3 * args.steps / (dev_ms / 1e3) / 1e6
+
+    # per-kernel event timing (separate run, same kernels, no graph)
+    rc = lib.nf_time_steps(solver._h, max(args.steps // 2, 2), 1, C.byref(ms), kms, kl)
+    if rc != 0:
+        raise RuntimeError(L.last_error(solver._h))
+    kern = {name: (kms[i] / max(kl[i], 1), int(kl[i])) for i, name in
+            ((L.NF_KERNEL_TIMESTEP, "timestep"), (L.NF_KERNEL_GRADIENT, "gradient"), (L.NF_KERNEL_FLUX, "flux"),
+             (L.NF_KERNEL_OTHER, "other"))}
+    nb = mesh.n_ghost
+    ab = algorithmic_bytes(N, mesh.n_faces, nb, args.precision)
+    hbm, hbm_kind = measured_peaks()
+    dom = max(("flux", "gradient"), key=lambda k: kern[k][0] * kern[k][1])
+    ach = ab[dom] / (kern[dom][0] * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(ach / hbm, 4), "peak_kind": hbm_kind, "traffic": None,
+            "algorithmic_bytes_per_launch": int(ab[dom]), "avg_launch_ms": round(kern[dom][0], 5),
+            "per_kernel_ms": {k: round(v[0], 5) for k, v in kern.items()}}
+    model = model_bytes_per_cell_stage(N, mesh.n_faces)
+    step_gbs = model * N * 3 * args.steps / (dev_ms / 1e3) / 1e9
+
+    # end to end through the public API: host state in, step, host state out
+    e2e = None
+    if not args.no_e2e:
+        pinned = torch.empty((N, 5), dtype=torch.float64, pin_memory=True).numpy()
+        pinned[:] = solver.get_solver_data().get_solution()
+        n_e = max(1, args.e2e_steps)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(n_e):
+            solver.set_state(pinned)
+            solver.calc_timestep(cfg)
+            solver.step(cfg)
+            rc = lib.nf_get_state(solver._h, L.dptr(pinned), N)
+            if rc != 0:
+                raise RuntimeError(L.last_error(solver._h))
+        wall = time.perf_counter() - t1
+        if dist:
+            t = torch.tensor([wall], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        e2e = {"value": round(world * N * 3 * n_e / wall / 1e6, 3), "unit": "Mcell-stages/s",
+               "h2d_bytes_per_step": int(N * 5 * 8), "d2h_bytes_per_step": int(N * 5 * 8 + 8),
+               "steps": n_e, "path": "EulerSolver.set_state/calc_timestep/step/get_state over the C ABI"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res = cpu_reference_baseline()
+        if res is not None:
+            cpu = {"value": round(res["all_cores"], 4), "unit": "Mcell-stages/s", "cores": res["cores"],
+                   "kind": "reference", "sample": res["sample"], "single_core": round(res["single_core"], 4)}
+
+    if rank == 0:
+        kernels_per_step = sum(kl) / max(args.steps // 2, 2)
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mcell-stages/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp64": "f64", "fp64_ref": "f64", "mixed": "f32+f64"}[args.precision],
+            "data": "synthetic",
+            "config": {"workload": desc, "cells": N, "faces": mesh.n_faces, "time_scheme": "TVD_RK3",
+                       "local_time_stepping": lts, "cfl": 0.8, "precision": args.precision,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "working set > 126 MB L2 (no flush needed)", "mesh_build_s": round(t_mesh, 2)},
+            "roofline": roof,
+            "step_roofline": {"model_bytes_per_cell_stage": round(model, 1), "achieved": round(step_gbs, 1),
+                              "peak": hbm, "unit": "GB/s", "frac": round(step_gbs / hbm, 4)},
+            "clocks": clocks.summary(),
+            "e2e": e2e,
+            "gpu_launches": int(round(kernels_per_step * args.steps)),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    solver.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -78,7 +78,8 @@ extern "C" {
 #define NF_FIELD_PRIMVARS 1   /* V of the last evaluated stage [N][5] (interior) */
 #define NF_FIELD_GRADIENT 2   /* grad V [N][15], entry (k,d) at 5*d+k as in the reference */
 #define NF_FIELD_LIMITER 3    /* Barth limiter [N][5] */
-#define NF_FIELD_FLUX_BALANCE 4 /* R of the last stage [N][5] (needs keep_flux_balance) */
+#define NF_FIELD_FLUX_BALANCE 4 /* R of the last stage [N][5] */
+/* GRADIENT, LIMITER and FLUX_BALANCE need nf_params.keep_stage_fields */
 #define NF_FIELD_LOCAL_DT 5   /* per-cell dt [N] (local time stepping) */
 
 typedef struct nf_mesh nf_mesh;
@@ -148,7 +149,8 @@ typedef struct {
   int dt_from_current_state; /* 0: dt from the primitives of the last
                                 evaluated stage, as the reference does
                                 (Solver.cpp:250); 1: from the current state */
-  int keep_flux_balance;     /* store R of every stage for nf_get_field */
+  int keep_stage_fields;     /* keep the gradient, limiter and flux balance of
+                                the last stage for nf_get_field */
   double cfl;
   double t_end;         /* > 0: nf_advance clips dt so time never passes t_end */
   /* Boundary conditions per patch of the mesh, in patch order. NULL: every
@@ -180,6 +182,23 @@ int nf_get_residual(nf_solver* s, double* rms_and_max, int n_cases);
 int nf_get_field(nf_solver* s, int which, double* out, int64_t n_values);
 /* Wait for queued work; report a device-side validity failure. */
 int nf_synchronize(nf_solver* s);
+
+/* Kernel classes reported by nf_time_steps. */
+#define NF_KERNEL_TIMESTEP 0
+#define NF_KERNEL_GRADIENT 1
+#define NF_KERNEL_FLUX 2
+#define NF_KERNEL_OTHER 3
+#define NF_KERNEL_COUNT 4
+
+/* Run n_steps (calc_timestep + step each) and time them with CUDA events on
+ * the solver's stream. per_kernel = 0: the steps run as in nf_advance (CUDA
+ * graph) and *ms_total is their device time. per_kernel = 1: every kernel is
+ * bracketed by events; kernel_ms[NF_KERNEL_COUNT] and
+ * kernel_launches[NF_KERNEL_COUNT] receive the summed time and launch count
+ * per kernel class. No counterpart in the reference (it has no timers beyond
+ * a wall clock around Driver::solve, Driver.cpp:27,59-60). */
+int nf_time_steps(nf_solver* s, int64_t n_steps, int per_kernel, double* ms_total, double* kernel_ms,
+                  int64_t* kernel_launches);
 const char* nf_last_error(const nf_solver* s);
 void nf_destroy(nf_solver* s);
 

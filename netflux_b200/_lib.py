@@ -30,7 +30,9 @@ EXPORTED = (
     "nf_mesh_export", "nf_mesh_get_permutation", "nf_mesh_get_case_offsets", "nf_mesh_destroy",
     "nf_params_default", "nf_create", "nf_set_state", "nf_get_state", "nf_calc_timestep", "nf_set_timestep",
     "nf_step", "nf_advance", "nf_get_residual", "nf_get_field", "nf_synchronize", "nf_last_error", "nf_destroy",
+    "nf_time_steps",
 )
+NF_KERNEL_TIMESTEP, NF_KERNEL_GRADIENT, NF_KERNEL_FLUX, NF_KERNEL_OTHER, NF_KERNEL_COUNT = range(5)
 
 
 class NfMeshInfo(C.Structure):
@@ -47,7 +49,7 @@ class NfPatchBC(C.Structure):
 class NfParams(C.Structure):
     _fields_ = [("time_scheme", C.c_int), ("spatial_order", C.c_int), ("limiter", C.c_int),
                 ("flux_scheme", C.c_int), ("precision", C.c_int), ("local_time_stepping", C.c_int),
-                ("dt_from_current_state", C.c_int), ("keep_flux_balance", C.c_int),
+                ("dt_from_current_state", C.c_int), ("keep_stage_fields", C.c_int),
                 ("cfl", C.c_double), ("t_end", C.c_double),
                 ("patches", C.POINTER(NfPatchBC)), ("n_patches", C.c_int),
                 ("freestream", C.c_double * 5), ("block_size", C.c_int)]
@@ -95,6 +97,7 @@ def load() -> C.CDLL:
         "nf_synchronize": (I, [P]),
         "nf_last_error": (C.c_char_p, [P]),
         "nf_destroy": (None, [P]),
+        "nf_time_steps": (I, [P, I64, I, dp, dp, i64p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -12,10 +12,15 @@
 //               (FV_Grid.cpp:135-137, 207-227), so every per-cell sum below
 //               adds the same terms in the same order as the face loops of
 //               Numerics.hpp:112-127 and Solver.cpp:171-229.
-//   face SoA    fi, fj : [F] owner / neighbour cell (fj < 0: boundary face of
-//               patch -fj-1); S, nhat, ri, rj : [3][F]; area : [F]
+//               nbslot : [4][stride] = neighbour << 2 | the neighbour's slot
+//               of the same face, or -(1 + patch) at a boundary face
+//   face states fs : [4][5][stride], the limited reconstruction of the cell's
+//               primitives at each of its faces (written by the gradient
+//               kernel, read by the flux kernel of both adjacent cells)
+//   face SoA    S, nhat, ri, rj : [3][F]; area : [F]
 // Each face's flux is evaluated by both of its cells with the owner on the
 // left, so both see bit-identical values; no atomics, deterministic results.
+// The gradient and flux kernels run four threads per cell (one per face slot).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -31,9 +36,8 @@ struct MeshView {
   int n;          // interior cells
   int stride;     // SoA stride of cell arrays
   int n_faces;
-  const int* __restrict__ slot;
-  const int* __restrict__ fi;
-  const int* __restrict__ fj;
+  const int* __restrict__ slot;    // [4][stride] face << 1 | side
+  const int* __restrict__ nbslot;  // [4][stride] neighbour << 2 | its slot, or -(1 + patch)
   const T* __restrict__ S;
   const T* __restrict__ nhat;
   const T* __restrict__ area;
@@ -51,8 +55,9 @@ struct StageArgs {
   int stage;             // 0, 1, 2
   int local_dt;
   const double* Vin;     // primitives of the stage input [5][stride]
-  double* grad;          // [15][stride]
-  double* phi;           // [5][stride]
+  double* fs;            // reconstructed face states [4 slots][5][stride]
+  double* grad;          // optional copy of the gradient [15][stride] (k*3+d)
+  double* phi;           // optional copy of the limiter [5][stride]
   const double* Uin;     // stage input state (own cell)
   const double* Un;      // U^n (stages 1, 2)
   double* Uout;          // may alias Uin
@@ -62,9 +67,10 @@ struct StageArgs {
   const double* dt_local;
   const double* scal;    // device scalars: [0] dt (min target), [1] time, [2] t_end
   unsigned* status;
-  // mixed precision: FP32 copies of the primitives and gradients
+  // mixed precision: FP32 copies of the primitives, face states and fields
   const float* Vin32;
   float* Vout32;
+  float* fs32;
   float* grad32;
   float* phi32;
 };
@@ -81,76 +87,137 @@ __device__ __forceinline__ double stage_dt(const double* scal) {
   return dt;
 }
 
+template <typename T>
+__device__ __forceinline__ T ld_v(const StageArgs& a, int idx) {
+  if constexpr (sizeof(T) == 8) return a.Vin[idx];
+  else return a.Vin32[idx];
+}
+
+// Four threads per cell: lane q of a quad owns the cell's face slot q. A
+// cell's per-face terms are combined across its quad with shuffles, folded in
+// slot order q = 0, 1, 2, 3, so sums keep the reference's order. A missing
+// slot contributes -0.0, which leaves any IEEE sum unchanged.
+constexpr unsigned kFull = 0xffffffffu;
+
+template <typename T>
+__device__ __forceinline__ T quad_sum_ordered(T v) {
+  T s = T(0);
+#pragma unroll
+  for (int p = 0; p < 4; p++) s = s + __shfl_sync(kFull, v, p, 4);
+  return s;
+}
+template <typename T>
+__device__ __forceinline__ T quad_max_ordered(T init, T v) {
+#pragma unroll
+  for (int p = 0; p < 4; p++) init = rmax(init, __shfl_sync(kFull, v, p, 4));
+  return init;
+}
+template <typename T>
+__device__ __forceinline__ T quad_min_ordered(T init, T v) {
+#pragma unroll
+  for (int p = 0; p < 4; p++) init = rmin(init, __shfl_sync(kFull, v, p, 4));
+  return init;
+}
+template <typename T>
+__device__ __forceinline__ T quad_sum_tree(T v) {
+  v = v + __shfl_xor_sync(kFull, v, 1, 4);
+  return v + __shfl_xor_sync(kFull, v, 2, 4);
+}
+template <typename T>
+__device__ __forceinline__ T quad_min_tree(T v) {
+  v = fmin(v, __shfl_xor_sync(kFull, v, 1, 4));
+  return fmin(v, __shfl_xor_sync(kFull, v, 2, 4));
+}
+template <typename T>
+__device__ __forceinline__ T quad_max_tree(T v) {
+  v = fmax(v, __shfl_xor_sync(kFull, v, 1, 4));
+  return fmax(v, __shfl_xor_sync(kFull, v, 2, 4));
+}
+
 // ---------------------------------------------------------------------------
 // Green-Gauss gradient + min/max + Barth limiter of one cell
 // (calc_green_gauss_gradient, calc_max_and_min_values, calc_barth_limiter,
-//  Numerics.hpp:86-292). Ghost states at boundary faces are the cell-centre
-// ghosts of set_constant_ghost_values (Solver.cpp:300-330).
+//  Numerics.hpp:86-292), then the limited reconstruction at each of its faces
+// (calc_limited_reconstruction, Numerics.hpp:135-145), which is what the flux
+// kernel consumes. Ghost states at boundary faces are the cell-centre ghosts
+// of set_constant_ghost_values (Solver.cpp:300-330).
 // ---------------------------------------------------------------------------
 template <typename T, bool kRef>
 __global__ void __launch_bounds__(256) gradient_limiter_kernel(MeshView<T> m, StageArgs a) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= m.n) return;
+  const int q = threadIdx.x & 3;
+  int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
+  const bool valid = c < m.n;
+  if (!valid) c = m.n - 1;  // every lane takes part in the quad shuffles
   const int st = m.stride;
+  const int F = m.n_faces;
   T Vc[5];
 #pragma unroll
-  for (int k = 0; k < 5; k++) {
-    if constexpr (sizeof(T) == 8) Vc[k] = T(a.Vin[k * st + c]);
-    else Vc[k] = a.Vin32[k * st + c];
-  }
+  for (int k = 0; k < 5; k++) Vc[k] = ld_v<T>(a, k * st + c);
   const T vol = T(m.vol[c]);
+  const int sl = m.slot[q * st + c];
+  const int ns = m.nbslot[q * st + c];
+  const bool has = sl >= 0;
+  const int f = has ? (sl >> 1) : 0;
+  const bool own = (sl & 1) == 0;
+
+  // this face's Green-Gauss term (reference: already divided by the volume)
+  // and its max/min candidates
+  T t[5][3], mx[5], mn[5];
+  if (has) {
+    const T S[3] = {m.S[f], m.S[F + f], m.S[2 * F + f]};
+    // the neighbour side of a face subtracts its term: (-x)/v == -(x/v) and
+    // g + (-y) == g - y exactly, so a signed normal reproduces both branches
+    const T Sg[3] = {own ? S[0] : -S[0], own ? S[1] : -S[1], own ? S[2] : -S[2]};
+    T Vo[5];
+    if (ns >= 0) {
+      const int o = ns >> 2;
+#pragma unroll
+      for (int k = 0; k < 5; k++) Vo[k] = ld_v<T>(a, k * st + o);
+    } else {
+      const T nh[3] = {m.nhat[f], m.nhat[F + f], m.nhat[2 * F + f]};
+      ghost_state<T>(m.patches[-ns - 1], Vc, nh, Vo);
+    }
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      const T uf = T(0.5) * (Vc[k] + Vo[k]);  // 0.5 (V_i + V_j); the sum commutes
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        if constexpr (kRef) t[k][d] = uf * Sg[d] / vol;
+        else t[k][d] = uf * Sg[d];
+      }
+      if constexpr (kRef) {
+        const T vi = own ? Vc[k] : Vo[k], vj = own ? Vo[k] : Vc[k];
+        mx[k] = rmax(vi, vj);
+        mn[k] = rmin(vi, vj);
+      } else {
+        mx[k] = Vo[k];
+        mn[k] = Vo[k];
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      t[k][0] = t[k][1] = t[k][2] = T(-0.0);
+      mx[k] = -std::numeric_limits<T>::max();
+      mn[k] = std::numeric_limits<T>::max();
+    }
+  }
+  // gradient of the cell: sum of the quad's terms
   T g[5][3];
   T vmax[5], vmin[5];
 #pragma unroll
   for (int k = 0; k < 5; k++) {
-    g[k][0] = g[k][1] = g[k][2] = T(0);
-    vmax[k] = -std::numeric_limits<T>::max();
-    vmin[k] = std::numeric_limits<T>::max();
-  }
-  T gsum[5][3];  // fast form: sum the face terms, divide once
-  if constexpr (!kRef) {
 #pragma unroll
-    for (int k = 0; k < 5; k++) gsum[k][0] = gsum[k][1] = gsum[k][2] = T(0);
-  }
-  int slots[4];
-#pragma unroll
-  for (int s = 0; s < 4; s++) slots[s] = m.slot[s * st + c];
-#pragma unroll
-  for (int s = 0; s < 4; s++) {
-    const int sl = slots[s];
-    if (sl < 0) continue;
-    const int f = sl >> 1;
-    const bool own = (sl & 1) == 0;
-    const T S[3] = {m.S[f], m.S[m.n_faces + f], m.S[2 * m.n_faces + f]};
-    const int o = own ? m.fj[f] : m.fi[f];
-    T Vo[5];
-    if (o >= 0) {
-#pragma unroll
-      for (int k = 0; k < 5; k++) {
-        if constexpr (sizeof(T) == 8) Vo[k] = T(a.Vin[k * st + o]);
-        else Vo[k] = a.Vin32[k * st + o];
-      }
-    } else {
-      const T nh[3] = {m.nhat[f], m.nhat[m.n_faces + f], m.nhat[2 * m.n_faces + f]};
-      ghost_state<T>(m.patches[-o - 1], Vc, nh, Vo);
+    for (int d = 0; d < 3; d++) {
+      if constexpr (kRef) g[k][d] = quad_sum_ordered(t[k][d]);
+      else g[k][d] = quad_sum_tree(t[k][d]);
     }
-#pragma unroll
-    for (int k = 0; k < 5; k++) {
-      // U_face = 0.5 * (V_i + V_j); the sum commutes exactly
-      const T uf = T(0.5) * (Vc[k] + Vo[k]);
-#pragma unroll
-      for (int d = 0; d < 3; d++) {
-        const T t = uf * S[d];
-        if constexpr (kRef) {
-          g[k][d] = own ? g[k][d] + t / vol : g[k][d] - t / vol;
-        } else {
-          gsum[k][d] = own ? gsum[k][d] + t : gsum[k][d] - t;
-        }
-      }
-      // max(V_i, V_j) / min(V_i, V_j) with the face's own operand order
-      const T vi = own ? Vc[k] : Vo[k], vj = own ? Vo[k] : Vc[k];
-      vmax[k] = rmax(vmax[k], rmax(vi, vj));
-      vmin[k] = rmin(vmin[k], rmin(vi, vj));
+    if constexpr (kRef) {
+      vmax[k] = quad_max_ordered(-std::numeric_limits<T>::max(), mx[k]);
+      vmin[k] = quad_min_ordered(std::numeric_limits<T>::max(), mn[k]);
+    } else {
+      vmax[k] = fmax(Vc[k], quad_max_tree(mx[k]));
+      vmin[k] = fmin(Vc[k], quad_min_tree(mn[k]));
     }
   }
   if constexpr (!kRef) {
@@ -158,71 +225,67 @@ __global__ void __launch_bounds__(256) gradient_limiter_kernel(MeshView<T> m, St
 #pragma unroll
     for (int k = 0; k < 5; k++)
 #pragma unroll
-      for (int d = 0; d < 3; d++) g[k][d] = gsum[k][d] * iv;
+      for (int d = 0; d < 3; d++) g[k][d] *= iv;
+  }
+  // grad V . r at this lane's face: the limiter's Delta_2 before its
+  // sign/epsilon adjustment, and the increment of the reconstruction
+  T gr[5];
+  {
+    const T* rr = own ? m.ri : m.rj;
+    const T r[3] = {rr[f], rr[F + f], rr[2 * F + f]};
+#pragma unroll
+    for (int k = 0; k < 5; k++) gr[k] = (g[k][0] * r[0] + g[k][1] * r[1]) + g[k][2] * r[2];
   }
   T phi[5];
   if (a.barth) {
 #pragma unroll
-    for (int k = 0; k < 5; k++) phi[k] = std::numeric_limits<T>::max();
-#pragma unroll
-    for (int s = 0; s < 4; s++) {
-      const int sl = slots[s];
-      if (sl < 0) continue;
-      const int f = sl >> 1;
-      const T* rr = (sl & 1) ? m.rj : m.ri;
-      const T r[3] = {rr[f], rr[m.n_faces + f], rr[2 * m.n_faces + f]};
-#pragma unroll
-      for (int k = 0; k < 5; k++) {
-        T d2 = (g[k][0] * r[0] + g[k][1] * r[1]) + g[k][2] * r[2];
+    for (int k = 0; k < 5; k++) {
+      T fc = std::numeric_limits<T>::max();  // identity of the min for an empty slot
+      if (has) {
+        T d2 = gr[k];
         const T sg = (d2 > T(0)) ? T(1) : ((d2 < T(0)) ? T(-1) : T(0));
         d2 = sg * (fabs(d2) + Gas<T>::eps);
-        T fc;
-        if (d2 > T(0)) fc = rmin(T(1), (vmax[k] - Vc[k]) / d2);
-        else if (d2 < T(0)) fc = rmin(T(1), (vmin[k] - Vc[k]) / d2);
-        else fc = T(1);
-        phi[k] = rmin(phi[k], fc);
+        if (d2 != T(0)) {
+          const T num = (d2 > T(0)) ? vmax[k] - Vc[k] : vmin[k] - Vc[k];
+          fc = rmin(T(1), num / d2);
+        } else {
+          fc = T(1);
+        }
       }
+      if constexpr (kRef) phi[k] = quad_min_ordered(std::numeric_limits<T>::max(), fc);
+      else phi[k] = quad_min_tree(fc);
     }
   } else {
 #pragma unroll
     for (int k = 0; k < 5; k++) phi[k] = T(1);
   }
-#pragma unroll
-  for (int k = 0; k < 5; k++) {
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      if constexpr (sizeof(T) == 8) a.grad[(k * 3 + d) * st + c] = g[k][d];
-      else a.grad32[(k * 3 + d) * st + c] = g[k][d];
-    }
-    if constexpr (sizeof(T) == 8) a.phi[k * st + c] = phi[k];
-    else a.phi32[k * st + c] = phi[k];
-  }
-}
-
-// Limited reconstruction V_face = V + phi (.) (grad V . r) (Numerics.hpp:135-145).
-template <typename T>
-__device__ __forceinline__ void reconstruct(const T V[5], const T g[5][3], const T phi[5], const T r[3], T out[5]) {
-#pragma unroll
-  for (int k = 0; k < 5; k++) out[k] = V[k] + phi[k] * ((g[k][0] * r[0] + g[k][1] * r[1]) + g[k][2] * r[2]);
-}
-
-template <typename T>
-__device__ __forceinline__ void load_cell(const StageArgs& a, int st, int c, bool second, T V[5], T g[5][3], T phi[5]) {
-#pragma unroll
-  for (int k = 0; k < 5; k++) {
-    if constexpr (sizeof(T) == 8) V[k] = a.Vin[k * st + c];
-    else V[k] = a.Vin32[k * st + c];
-  }
-  if (second) {
+  if (valid && has) {
 #pragma unroll
     for (int k = 0; k < 5; k++) {
+      const T v = Vc[k] + phi[k] * gr[k];
+      if constexpr (sizeof(T) == 8) a.fs[(q * 5 + k) * st + c] = v;
+      else a.fs32[(q * 5 + k) * st + c] = v;
+    }
+  }
+  if (valid && q == 0) {
+    if constexpr (sizeof(T) == 8) {
+      if (a.grad) {
 #pragma unroll
-      for (int d = 0; d < 3; d++) {
-        if constexpr (sizeof(T) == 8) g[k][d] = a.grad[(k * 3 + d) * st + c];
-        else g[k][d] = a.grad32[(k * 3 + d) * st + c];
+        for (int k = 0; k < 5; k++) {
+#pragma unroll
+          for (int d = 0; d < 3; d++) a.grad[(k * 3 + d) * st + c] = g[k][d];
+          a.phi[k * st + c] = phi[k];
+        }
       }
-      if constexpr (sizeof(T) == 8) phi[k] = a.phi[k * st + c];
-      else phi[k] = a.phi32[k * st + c];
+    } else {
+      if (a.grad32) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+#pragma unroll
+          for (int d = 0; d < 3; d++) a.grad32[(k * 3 + d) * st + c] = g[k][d];
+          a.phi32[k * st + c] = phi[k];
+        }
+      }
     }
   }
 }
@@ -232,64 +295,74 @@ __device__ __forceinline__ void load_cell(const StageArgs& a, int st, int c, boo
 // (evaluate_inviscid_fluxes Solver.cpp:144-230, rusanov Numerics.cpp:10-18,
 //  TVD_RK3 Solver.cpp:103-133, explicit_euler 83-101), then the primitives of
 // the new state for the next stage (set_primvars, SolverData.cpp:37-48).
+// The face states come from gradient_limiter_kernel (second order) or are the
+// cell primitives (first order). Lane q evaluates the flux of face slot q.
 // ---------------------------------------------------------------------------
 template <typename T, bool kRef>
 __global__ void __launch_bounds__(256) flux_update_kernel(MeshView<T> m, StageArgs a) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= m.n) return;
+  const int q = threadIdx.x & 3;
+  int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
+  const bool valid = c < m.n;
+  if (!valid) c = m.n - 1;
   const int st = m.stride;
+  const int F = m.n_faces;
   const bool second = a.second_order != 0;
-  T Vc[5], gc[5][3], phic[5];
-  load_cell<T>(a, st, c, second, Vc, gc, phic);
-  double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll 1
-  for (int s = 0; s < 4; s++) {
-    const int sl = m.slot[s * st + c];
-    if (sl < 0) continue;
+  const int sl = m.slot[q * st + c];
+  const int ns = m.nbslot[q * st + c];
+  const bool has = sl >= 0;
+  const bool own = (sl & 1) == 0;
+  // this face's contribution to R: -F on the owner side, +F on the other
+  double contrib[5] = {-0.0, -0.0, -0.0, -0.0, -0.0};
+  if (has) {
     const int f = sl >> 1;
-    const bool own = (sl & 1) == 0;
-    const T nh[3] = {m.nhat[f], m.nhat[m.n_faces + f], m.nhat[2 * m.n_faces + f]};
+    const T nh[3] = {m.nhat[f], m.nhat[F + f], m.nhat[2 * F + f]};
     const T area = m.area[f];
-    T VL[5], VR[5];
-    const T* rc = own ? m.ri : m.rj;  // this cell's centroid-to-face vector
-    const T r_own[3] = {rc[f], rc[m.n_faces + f], rc[2 * m.n_faces + f]};
-    T* Vown = own ? VL : VR;
-    T* Voth = own ? VR : VL;
-    if (second) reconstruct<T>(Vc, gc, phic, r_own, Vown);
-    else {
+    T Vs[5], Vx[5];  // this cell's face state, the other side's
 #pragma unroll
-      for (int k = 0; k < 5; k++) Vown[k] = Vc[k];
-    }
-    const int o = own ? m.fj[f] : m.fi[f];
-    if (o >= 0) {
-      T Vo[5], go[5][3], phio[5];
-      load_cell<T>(a, st, o, second, Vo, go, phio);
+    for (int k = 0; k < 5; k++) {
       if (second) {
-        const T* ro = own ? m.rj : m.ri;
-        const T r_oth[3] = {ro[f], ro[m.n_faces + f], ro[2 * m.n_faces + f]};
-        reconstruct<T>(Vo, go, phio, r_oth, Voth);
+        if constexpr (sizeof(T) == 8) Vs[k] = a.fs[(q * 5 + k) * st + c];
+        else Vs[k] = a.fs32[(q * 5 + k) * st + c];
       } else {
+        Vs[k] = ld_v<T>(a, k * st + c);
+      }
+    }
+    if (ns >= 0) {
+      const int o = ns >> 2, q2 = ns & 3;
 #pragma unroll
-        for (int k = 0; k < 5; k++) Voth[k] = Vo[k];
+      for (int k = 0; k < 5; k++) {
+        if (second) {
+          if constexpr (sizeof(T) == 8) Vx[k] = a.fs[(q2 * 5 + k) * st + o];
+          else Vx[k] = a.fs32[(q2 * 5 + k) * st + o];
+        } else {
+          Vx[k] = ld_v<T>(a, k * st + o);
+        }
       }
     } else {
-      // boundary face: ghost from the reconstructed face value (Solver.cpp:212)
-      ghost_state<T>(m.patches[-o - 1], VL, nh, VR);
+      // boundary face (this cell is its owner): ghost from the reconstructed
+      // face value (Solver.cpp:212)
+      ghost_state<T>(m.patches[-ns - 1], Vs, nh, Vx);
     }
-    T F[5];
+    const T* VL = own ? Vs : Vx;
+    const T* VR = own ? Vx : Vs;
+    T Fl[5];
     if constexpr (kRef) {
       T UL[5], UR[5];
       prim_to_cons<T, kRef>(VL, UL);
       prim_to_cons<T, kRef>(VR, UR);
-      rusanov_ref<T>(UL, UR, nh, area, F);
+      rusanov_ref<T>(UL, UR, nh, area, Fl);
     } else {
-      rusanov_fast<T>(VL, VR, nh, area, F);
+      rusanov_fast<T>(VL, VR, nh, area, Fl);
     }
 #pragma unroll
-    for (int k = 0; k < 5; k++) R[k] = own ? R[k] - double(F[k]) : R[k] + double(F[k]);
+    for (int k = 0; k < 5; k++) contrib[k] = own ? -double(Fl[k]) : double(Fl[k]);
   }
+  // flux balance, accumulated in face-slot order: ((0 + c0) + c1) + ...
+  double R[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) R[k] = quad_sum_ordered(contrib[k]);
 
-  // ---- stage update (FP64) ----
+  // ---- stage update (FP64); every lane computes it, lanes store by component ----
   const double vol = m.vol[c];
   const double dt = a.local_dt ? a.dt_local[c] : stage_dt(a.scal);
   double U[5], Uo[5];
@@ -301,35 +374,38 @@ __global__ void __launch_bounds__(256) flux_update_kernel(MeshView<T> m, StageAr
   }
   double Unew[5];
   if (a.scheme == 0 || a.stage == 0) {
-    const double q = dt / vol;
+    const double qf = dt / vol;
 #pragma unroll
-    for (int k = 0; k < 5; k++) Unew[k] = U[k] + q * R[k];
+    for (int k = 0; k < 5; k++) Unew[k] = U[k] + qf * R[k];
   } else if (a.stage == 1) {
-    const double q = 1.0 / 4.0 * dt / vol;
+    const double qf = 1.0 / 4.0 * dt / vol;
 #pragma unroll
-    for (int k = 0; k < 5; k++) Unew[k] = 3.0 / 4.0 * Uo[k] + 1.0 / 4.0 * U[k] + q * R[k];
+    for (int k = 0; k < 5; k++) Unew[k] = 3.0 / 4.0 * Uo[k] + 1.0 / 4.0 * U[k] + qf * R[k];
   } else {
-    const double q = 2.0 / 3.0 * dt / vol;
+    const double qf = 2.0 / 3.0 * dt / vol;
 #pragma unroll
-    for (int k = 0; k < 5; k++) Unew[k] = 1.0 / 3.0 * Uo[k] + 2.0 / 3.0 * U[k] + q * R[k];
+    for (int k = 0; k < 5; k++) Unew[k] = 1.0 / 3.0 * Uo[k] + 2.0 / 3.0 * U[k] + qf * R[k];
   }
   double Vn[5];
   cons_to_prim<double, kRef>(Unew, Vn);
-  bool finite = true;
+  if (!valid) return;
 #pragma unroll
   for (int k = 0; k < 5; k++) {
-    a.Uout[k * st + c] = Unew[k];
-    a.Vout[k * st + c] = Vn[k];
-    if (a.Vout32) a.Vout32[k * st + c] = float(Vn[k]);
-    finite = finite && isfinite(R[k]) && isfinite(Unew[k]);
+    if (k == q || (k == 4 && q == 0)) {
+      a.Uout[k * st + c] = Unew[k];
+      a.Vout[k * st + c] = Vn[k];
+      if (a.Vout32) a.Vout32[k * st + c] = float(Vn[k]);
+      if (a.R) a.R[k * st + c] = R[k];
+    }
   }
-  if (a.R) {
+  if (q == 0) {
+    if (a.res_cell) a.res_cell[c] = R[0] / vol;
+    bool finite = true;
 #pragma unroll
-    for (int k = 0; k < 5; k++) a.R[k * st + c] = R[k];
+    for (int k = 0; k < 5; k++) finite = finite && isfinite(R[k]) && isfinite(Unew[k]);
+    if (!finite) atomicOr(a.status, kErrNonFinite);
+    else if (!(Vn[0] > 0.0) || !(Vn[4] > 0.0)) atomicOr(a.status, kErrNonPhysical);
   }
-  if (a.res_cell) a.res_cell[c] = R[0] / vol;
-  if (!finite) atomicOr(a.status, kErrNonFinite);
-  else if (!(Vn[0] > 0.0) || !(Vn[4] > 0.0)) atomicOr(a.status, kErrNonPhysical);
 }
 
 // ---------------------------------------------------------------------------

@@ -23,16 +23,16 @@ __global__ void __launch_bounds__(256) prim_kernel_fast(int n, int st, const dou
 static inline int grid_for(int n, int block) { return (n + block - 1) / block; }
 
 void launch_gradient_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
-  gradient_limiter_kernel<double, false><<<grid_for(m.n, l.block), l.block, 0, l.stream>>>(m, a);
+  gradient_limiter_kernel<double, false><<<grid_for(4 * m.n, l.block), l.block, 0, l.stream>>>(m, a);
 }
 void launch_flux_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
-  flux_update_kernel<double, false><<<grid_for(m.n, l.block), l.block, 0, l.stream>>>(m, a);
+  flux_update_kernel<double, false><<<grid_for(4 * m.n, l.block), l.block, 0, l.stream>>>(m, a);
 }
 void launch_gradient_mixed(const MeshView<float>& m, const StageArgs& a, Launch l) {
-  gradient_limiter_kernel<float, false><<<grid_for(m.n, l.block), l.block, 0, l.stream>>>(m, a);
+  gradient_limiter_kernel<float, false><<<grid_for(4 * m.n, l.block), l.block, 0, l.stream>>>(m, a);
 }
 void launch_flux_mixed(const MeshView<float>& m, const StageArgs& a, Launch l) {
-  flux_update_kernel<float, false><<<grid_for(m.n, l.block), l.block, 0, l.stream>>>(m, a);
+  flux_update_kernel<float, false><<<grid_for(4 * m.n, l.block), l.block, 0, l.stream>>>(m, a);
 }
 void launch_prim_fast(int n, int stride, const double* U, double* V, float* V32, Launch l) {
   prim_kernel_fast<false><<<grid_for(n, l.block), l.block, 0, l.stream>>>(n, stride, U, V, V32);

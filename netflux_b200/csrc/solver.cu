@@ -69,8 +69,11 @@ __global__ void scal_kernel(double* scal, int op, unsigned* status) {
   if (op == 0) {  // reset the dt minimum before the timestep kernel
     scal[kScalDtMin] = DBL_MAX;
   } else {  // end of step: time += dt actually used
+    // the computed dt must be valid (Solver.cpp:267-268); the dt clipped at
+    // t_end may be 0 once the end time is reached
+    const double raw = scal[kScalDtMin];
+    if (!(raw > 0.0) || !isfinite(raw)) atomicOr(status, kErrDt);
     const double dt = stage_dt(scal);
-    if (!(dt > 0.0) || !isfinite(dt)) atomicOr(status, kErrDt);
     scal[kScalDtUsed] = dt;
     scal[kScalTime] = scal[kScalTime] + dt;
   }
@@ -120,6 +123,25 @@ __global__ void residual_finalize_kernel(const double* __restrict__ part, const 
   out[2 * cs + 1] = mx;
 }
 
+// AoS state in reference cell order <-> SoA in device order.
+__global__ void scatter_state_kernel(int n, int st, const long long* __restrict__ dev_of_ref,
+                                     const double* __restrict__ aos, double* __restrict__ soa) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const long long d = dev_of_ref[c];
+#pragma unroll
+  for (int k = 0; k < 5; k++) soa[k * st + d] = aos[5 * (long long)c + k];
+}
+
+__global__ void gather_state_kernel(int n, int st, const long long* __restrict__ dev_of_ref,
+                                    const double* __restrict__ soa, double* __restrict__ aos) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const long long d = dev_of_ref[c];
+#pragma unroll
+  for (int k = 0; k < 5; k++) aos[5 * (long long)c + k] = soa[k * st + d];
+}
+
 }  // namespace
 
 struct nf_solver {
@@ -133,13 +155,13 @@ struct nf_solver {
   std::string err;
 
   // mesh
-  DevBuf<int> slot, fi, fj;
+  DevBuf<int> slot, nbslot;
   DevBuf<double> S, nhat, area, ri, rj, vol, dS;
   DevBuf<float> S32, nhat32, area32, ri32, rj32;
   DevBuf<nf::PatchBC> patches;
   // state
-  DevBuf<double> U, W, V0, V1, grad, phi, R, dt_local, res_cell, scal, part, res_out;
-  DevBuf<float> V32a, V32b, grad32, phi32;
+  DevBuf<double> U, W, V0, V1, fs, grad, phi, R, dt_local, res_cell, scal, part, res_out;
+  DevBuf<float> V32a, V32b, fs32, grad32, phi32;
   DevBuf<unsigned> status;
   DevBuf<long long> chunk_begin, chunk_end, case_cells;
   DevBuf<int> case_chunk0;
@@ -148,22 +170,50 @@ struct nf_solver {
   int vcur = 0;              // V buffer holding the primitives of the current state
   bool stepped = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two steps from vcur = 0 / 1
+  DevBuf<double> stage;           // AoS staging for state transfers [N][5]
+  DevBuf<long long> d_dev_of_ref;  // [N]
+
+  // per-kernel timing: events around every launch while prof_on
+  bool prof_on = false;
+  std::vector<cudaEvent_t> prof_ev;
+  std::vector<int> prof_cls;
+  size_t prof_used = 0;
+  void prof_begin(int cls) {
+    if (!prof_on) return;
+    if (2 * prof_used + 2 > prof_ev.size()) {
+      for (int k = 0; k < 64; k++) {
+        cudaEvent_t e;
+        ck(cudaEventCreate(&e), "cudaEventCreate");
+        prof_ev.push_back(e);
+      }
+    }
+    if (prof_cls.size() <= prof_used) prof_cls.resize(prof_used + 1);
+    prof_cls[prof_used] = cls;
+    ck(cudaEventRecord(prof_ev[2 * prof_used], stream), "cudaEventRecord");
+  }
+  void prof_end() {
+    if (!prof_on) return;
+    ck(cudaEventRecord(prof_ev[2 * prof_used + 1], stream), "cudaEventRecord");
+    prof_used++;
+  }
 
   double* Vbuf(int i) { return i ? V1.p : V0.p; }
   float* V32buf(int i) { return i ? V32b.p : V32a.p; }
   nf::Launch launch() const { return nf::Launch{block, stream}; }
 
   nf::MeshView<double> view64() const {
-    return nf::MeshView<double>{n, stride, n_faces, slot.p, fi.p, fj.p, S.p, nhat.p, area.p, ri.p, rj.p,
+    return nf::MeshView<double>{n, stride, n_faces, slot.p, nbslot.p, S.p, nhat.p, area.p, ri.p, rj.p,
                                 vol.p, dS.p, patches.p};
   }
   nf::MeshView<float> view32() const {
-    return nf::MeshView<float>{n, stride, n_faces, slot.p, fi.p, fj.p, S32.p, nhat32.p, area32.p, ri32.p, rj32.p,
+    return nf::MeshView<float>{n, stride, n_faces, slot.p, nbslot.p, S32.p, nhat32.p, area32.p, ri32.p, rj32.p,
                                vol.p, dS.p, patches.p};
   }
 
   void enqueue_dt() {
+    prof_begin(NF_KERNEL_OTHER);
     scal_kernel<<<1, 1, 0, stream>>>(scal.p, 0, status.p);
+    prof_end();
     nf::DtArgs a;
     const int vb = p.dt_from_current_state ? vcur : (stepped ? 1 - vcur : vcur);
     a.V = Vbuf(vb);
@@ -171,7 +221,9 @@ struct nf_solver {
     a.dt_local = p.local_time_stepping ? dt_local.p : nullptr;
     a.dt_min_bits = reinterpret_cast<unsigned long long*>(scal.p + nf::kScalDtMin);
     a.status = status.p;
+    prof_begin(NF_KERNEL_TIMESTEP);
     nf::launch_timestep(view64(), a, launch());
+    prof_end();
   }
 
   void enqueue_step() {
@@ -185,9 +237,10 @@ struct nf_solver {
       a.local_dt = p.local_time_stepping;
       a.Vin = Vbuf(vcur);
       a.Vout = Vbuf(1 - vcur);
-      a.grad = grad.p;
-      a.phi = phi.p;
-      a.R = p.keep_flux_balance ? R.p : nullptr;
+      a.fs = fs.p;
+      a.grad = p.keep_stage_fields ? grad.p : nullptr;
+      a.phi = p.keep_stage_fields ? phi.p : nullptr;
+      a.R = p.keep_stage_fields ? R.p : nullptr;
       a.res_cell = s == 0 ? res_cell.p : nullptr;
       a.dt_local = dt_local.p;
       a.scal = scal.p;
@@ -210,20 +263,27 @@ struct nf_solver {
       if (p.precision == NF_PREC_MIXED) {
         a.Vin32 = V32buf(vcur);
         a.Vout32 = V32buf(1 - vcur);
-        a.grad32 = grad32.p;
-        a.phi32 = phi32.p;
-        if (a.second_order) nf::launch_gradient_mixed(view32(), a, launch());
-        nf::launch_flux_mixed(view32(), a, launch());
-      } else if (p.precision == NF_PREC_FP64) {
-        if (a.second_order) nf::launch_gradient_fast(view64(), a, launch());
-        nf::launch_flux_fast(view64(), a, launch());
-      } else {
-        if (a.second_order) nf::launch_gradient_ref(view64(), a, launch());
-        nf::launch_flux_ref(view64(), a, launch());
+        a.fs32 = fs32.p;
+        a.grad32 = p.keep_stage_fields ? grad32.p : nullptr;
+        a.phi32 = p.keep_stage_fields ? phi32.p : nullptr;
       }
+      if (a.second_order) {
+        prof_begin(NF_KERNEL_GRADIENT);
+        if (p.precision == NF_PREC_MIXED) nf::launch_gradient_mixed(view32(), a, launch());
+        else if (p.precision == NF_PREC_FP64) nf::launch_gradient_fast(view64(), a, launch());
+        else nf::launch_gradient_ref(view64(), a, launch());
+        prof_end();
+      }
+      prof_begin(NF_KERNEL_FLUX);
+      if (p.precision == NF_PREC_MIXED) nf::launch_flux_mixed(view32(), a, launch());
+      else if (p.precision == NF_PREC_FP64) nf::launch_flux_fast(view64(), a, launch());
+      else nf::launch_flux_ref(view64(), a, launch());
+      prof_end();
       vcur = 1 - vcur;
     }
+    prof_begin(NF_KERNEL_OTHER);
     scal_kernel<<<1, 1, 0, stream>>>(scal.p, 1, status.p);
+    prof_end();
     stepped = true;
   }
 
@@ -251,6 +311,7 @@ struct nf_solver {
   ~nf_solver() {
     for (auto& g : graph)
       if (g) cudaGraphExecDestroy(g);
+    for (auto e : prof_ev) cudaEventDestroy(e);
     if (h_scal) cudaFreeHost(h_scal);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -474,14 +535,10 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     std::vector<int64_t> fdev(static_cast<size_t>(F));
     for (int64_t k = 0; k < F; k++) fdev[size_t(dev_face_order[size_t(k)])] = k;
 
-    std::vector<int> h_fi(static_cast<size_t>(F)), h_fj(static_cast<size_t>(F));
     std::vector<double> h_S(size_t(3 * F)), h_n(size_t(3 * F)), h_a(static_cast<size_t>(F)), h_ri(size_t(3 * F)),
         h_rj(size_t(3 * F));
     for (int64_t f = 0; f < F; f++) {
       const int64_t d = fdev[size_t(f)];
-      h_fi[size_t(d)] = int(m.dev_of_ref[m.face_i[size_t(f)]]);
-      const uint32_t j = m.face_j[size_t(f)];
-      h_fj[size_t(d)] = j < uint32_t(N) ? int(m.dev_of_ref[j]) : -(1 + m.face_patch[size_t(f)]);
       h_a[size_t(d)] = m.area[size_t(f)];
       for (int c = 0; c < 3; c++) {
         h_S[size_t(c * F + d)] = m.S[size_t(3 * f + c)];
@@ -490,20 +547,28 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
         h_rj[size_t(c * F + d)] = m.rj[size_t(3 * f + c)];
       }
     }
-    // slots in reference face order
-    std::vector<int> h_slot(size_t(4) * stride, -1);
-    std::vector<int> fill(size_t(stride), 0);
+    // slots in reference face order; nbslot names the other side of each face
+    std::vector<int> h_slot(size_t(4) * stride, -1), h_nb(size_t(4) * stride, 0);
+    std::vector<int> fill(static_cast<size_t>(stride), 0);
     auto add_slot = [&](int64_t cell_dev, int value) {
       int& k = fill[size_t(cell_dev)];
       if (k >= 4) throw std::runtime_error("a cell has more than 4 faces (only tetrahedra are supported)");
       h_slot[size_t(k) * stride + size_t(cell_dev)] = value;
-      k++;
+      return k++;
     };
     for (int64_t f = 0; f < F; f++) {
       const int fd = int(fdev[size_t(f)]);
-      add_slot(m.dev_of_ref[m.face_i[size_t(f)]], fd << 1);
+      const int64_t di = m.dev_of_ref[m.face_i[size_t(f)]];
+      const int qi = add_slot(di, fd << 1);
       const uint32_t j = m.face_j[size_t(f)];
-      if (j < uint32_t(N)) add_slot(m.dev_of_ref[j], (fd << 1) | 1);
+      if (j < uint32_t(N)) {
+        const int64_t dj = m.dev_of_ref[j];
+        const int qj = add_slot(dj, (fd << 1) | 1);
+        h_nb[size_t(qi) * stride + size_t(di)] = int(dj << 2) | qj;
+        h_nb[size_t(qj) * stride + size_t(dj)] = int(di << 2) | qi;
+      } else {
+        h_nb[size_t(qi) * stride + size_t(di)] = -(1 + m.face_patch[size_t(f)]);
+      }
     }
     std::vector<double> h_vol(size_t(stride), 1.0), h_dS(size_t(3) * stride, 0.0);
     for (int64_t c = 0; c < N; c++) {
@@ -525,9 +590,8 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
       if (b.type < 0 || b.type > 2) throw std::runtime_error("bad boundary type");
     }
 
-    s->fi.upload(h_fi, st);
-    s->fj.upload(h_fj, st);
     s->slot.upload(h_slot, st);
+    s->nbslot.upload(h_nb, st);
     s->S.upload(h_S, st);
     s->nhat.upload(h_n, st);
     s->area.upload(h_a, st);
@@ -549,28 +613,40 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
       s->rj32.upload(tof(h_rj), st);
       s->V32a.alloc(size_t(5) * stride);
       s->V32b.alloc(size_t(5) * stride);
-      s->grad32.alloc(size_t(15) * stride);
-      s->phi32.alloc(size_t(5) * stride);
+      s->fs32.alloc(size_t(20) * stride);
       s->V32a.zero(st);
       s->V32b.zero(st);
-      s->grad32.zero(st);
-      s->phi32.zero(st);
+      s->fs32.zero(st);
+      if (p.keep_stage_fields) {
+        s->grad32.alloc(size_t(15) * stride);
+        s->phi32.alloc(size_t(5) * stride);
+        s->grad32.zero(st);
+        s->phi32.zero(st);
+      }
     }
     s->U.alloc(size_t(5) * stride);
     s->W.alloc(size_t(5) * stride);
     s->V0.alloc(size_t(5) * stride);
     s->V1.alloc(size_t(5) * stride);
-    s->grad.alloc(size_t(15) * stride);
-    s->phi.alloc(size_t(5) * stride);
-    if (p.keep_flux_balance) {
+    if (p.precision != NF_PREC_MIXED) {
+      s->fs.alloc(size_t(20) * stride);
+      s->fs.zero(st);
+    }
+    if (p.keep_stage_fields) {
       s->R.alloc(size_t(5) * stride);
       s->R.zero(st);
+      if (p.precision != NF_PREC_MIXED) {
+        s->grad.alloc(size_t(15) * stride);
+        s->phi.alloc(size_t(5) * stride);
+        s->grad.zero(st);
+        s->phi.zero(st);
+      }
     }
     s->dt_local.alloc(static_cast<size_t>(stride));
     s->res_cell.alloc(static_cast<size_t>(stride));
     s->scal.alloc(nf::kScalCount);
     s->status.alloc(1);
-    for (auto* b : {&s->U, &s->W, &s->V0, &s->V1, &s->grad, &s->phi, &s->dt_local, &s->res_cell, &s->scal})
+    for (auto* b : {&s->U, &s->W, &s->V0, &s->V1, &s->dt_local, &s->res_cell, &s->scal})
       b->zero(st);
     s->status.zero(st);
     // residual chunks: fixed-size pieces of each case's cell range
@@ -596,6 +672,11 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     s->case_cells.upload(cc, st);
     s->case_chunk0.upload(c0, st);
     s->part.alloc(size_t(2) * s->n_chunks);
+    s->stage.alloc(size_t(5) * N);
+    {
+      std::vector<long long> dor(m.dev_of_ref.begin(), m.dev_of_ref.end());
+      s->d_dev_of_ref.upload(dor, st);
+    }
     s->res_out.alloc(size_t(2) * s->n_cases);
     ck(cudaMallocHost(&s->h_scal, nf::kScalCount * sizeof(double)), "cudaMallocHost");
     std::fill(s->h_scal, s->h_scal + nf::kScalCount, 0.0);
@@ -618,21 +699,16 @@ int nf_set_state(nf_solver* s, const double* U, int64_t n_cells) {
       return NF_ERR_ARG;
     }
     const int st = s->stride;
-    std::vector<double> h(size_t(5) * st, 0.0);
-    for (int64_t c = 0; c < n_cells; c++) {
-      const int64_t d = s->dev_of_ref[size_t(c)];
-      for (int k = 0; k < 5; k++) h[size_t(k) * st + size_t(d)] = U[5 * c + k];
-    }
-    ck(cudaMemcpyAsync(s->U.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream), "U H2D");
+    // one copy of the caller's AoS array, then a permutation kernel into SoA
+    ck(cudaMemcpyAsync(s->stage.p, U, size_t(5) * s->n * sizeof(double), cudaMemcpyHostToDevice, s->stream),
+       "U H2D");
+    scatter_state_kernel<<<(s->n + 255) / 256, 256, 0, s->stream>>>(s->n, st, s->d_dev_of_ref.p, s->stage.p, s->U.p);
     // primitives of the initial state in both buffers (the first
     // calc_timestep reads them, like the harness-initialised reference)
     for (int b = 0; b < 2; b++) {
-      if (s->p.precision == NF_PREC_FP64_REF)
-        nf::launch_prim_ref(s->n, st, s->U.p, s->Vbuf(b), s->p.precision == NF_PREC_MIXED ? s->V32buf(b) : nullptr,
-                            s->launch());
-      else
-        nf::launch_prim_fast(s->n, st, s->U.p, s->Vbuf(b),
-                             s->p.precision == NF_PREC_MIXED ? s->V32buf(b) : nullptr, s->launch());
+      float* v32 = s->p.precision == NF_PREC_MIXED ? s->V32buf(b) : nullptr;
+      if (s->p.precision == NF_PREC_FP64_REF) nf::launch_prim_ref(s->n, st, s->U.p, s->Vbuf(b), v32, s->launch());
+      else nf::launch_prim_fast(s->n, st, s->U.p, s->Vbuf(b), v32, s->launch());
     }
     s->vcur = 0;
     s->stepped = false;
@@ -649,14 +725,11 @@ int nf_get_state(nf_solver* s, double* U, int64_t n_cells) {
       s->err = "nf_get_state: state size does not match the mesh";
       return NF_ERR_ARG;
     }
-    const int st = s->stride;
-    std::vector<double> h(size_t(5) * st);
-    ck(cudaMemcpyAsync(h.data(), s->U.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "U D2H");
+    gather_state_kernel<<<(s->n + 255) / 256, 256, 0, s->stream>>>(s->n, s->stride, s->d_dev_of_ref.p, s->U.p,
+                                                                   s->stage.p);
+    ck(cudaMemcpyAsync(U, s->stage.p, size_t(5) * s->n * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
+       "U D2H");
     ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
-    for (int64_t c = 0; c < n_cells; c++) {
-      const int64_t d = s->dev_of_ref[size_t(c)];
-      for (int k = 0; k < 5; k++) U[5 * c + k] = h[size_t(k) * st + size_t(d)];
-    }
     return s->check_status();
   });
 }
@@ -778,7 +851,7 @@ int nf_get_field(nf_solver* s, int which, double* out, int64_t n_values) {
       default: s->err = "nf_get_field: unknown field"; return NF_ERR_ARG;
     }
     if (!src) {
-      s->err = "nf_get_field: field not kept (set keep_flux_balance)";
+      s->err = "nf_get_field: field not kept (set keep_stage_fields)";
       return NF_ERR_ARG;
     }
     if (!out || n_values != int64_t(comps) * s->n) {
@@ -787,6 +860,10 @@ int nf_get_field(nf_solver* s, int which, double* out, int64_t n_values) {
     }
     std::vector<double> h(size_t(comps) * st);
     if (s->p.precision == NF_PREC_MIXED && (which == NF_FIELD_GRADIENT || which == NF_FIELD_LIMITER)) {
+      if (!s->grad32.p) {
+        s->err = "nf_get_field: field not kept (set keep_stage_fields)";
+        return NF_ERR_ARG;
+      }
       std::vector<float> hf(size_t(comps) * st);
       const float* src32 = which == NF_FIELD_GRADIENT ? s->grad32.p : s->phi32.p;
       ck(cudaMemcpyAsync(hf.data(), src32, hf.size() * sizeof(float), cudaMemcpyDeviceToHost, s->stream), "D2H");
@@ -807,6 +884,70 @@ int nf_get_field(nf_solver* s, int which, double* out, int64_t n_values) {
       }
     }
     return NF_OK;
+  });
+}
+
+int nf_time_steps(nf_solver* s, int64_t n_steps, int per_kernel, double* ms_total, double* kernel_ms,
+                  int64_t* kernel_launches) {
+  return guarded(s, [&]() -> int {
+    if (n_steps <= 0 || !ms_total) return NF_ERR_ARG;
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "cudaEventCreate");
+    ck(cudaEventCreate(&e1), "cudaEventCreate");
+    ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
+    if (per_kernel) {
+      s->prof_on = true;
+      s->prof_used = 0;
+    }
+    ck(cudaEventRecord(e0, s->stream), "cudaEventRecord");
+    int64_t left = n_steps;
+    if (!per_kernel && left >= 2 && s->stepped) {
+      const int v0 = s->vcur;
+      if (!s->graph[v0]) {
+        cudaGraph_t g = nullptr;
+        ck(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        for (int k = 0; k < 2; k++) {
+          s->enqueue_dt();
+          s->enqueue_step();
+        }
+        ck(cudaStreamEndCapture(s->stream, &g), "end capture");
+        ck(cudaGraphInstantiate(&s->graph[v0], g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
+        s->vcur = v0;
+        // instantiation happened inside the timed region: restart the clock
+        ck(cudaEventRecord(e0, s->stream), "cudaEventRecord");
+      }
+      while (left >= 2) {
+        ck(cudaGraphLaunch(s->graph[v0], s->stream), "graph launch");
+        left -= 2;
+      }
+    }
+    while (left > 0) {
+      s->enqueue_dt();
+      s->enqueue_step();
+      left--;
+    }
+    ck(cudaEventRecord(e1, s->stream), "cudaEventRecord");
+    ck(cudaEventSynchronize(e1), "cudaEventSynchronize");
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+    *ms_total = ms;
+    if (per_kernel) {
+      s->prof_on = false;
+      if (kernel_ms)
+        for (int k = 0; k < NF_KERNEL_COUNT; k++) kernel_ms[k] = 0.0;
+      if (kernel_launches)
+        for (int k = 0; k < NF_KERNEL_COUNT; k++) kernel_launches[k] = 0;
+      for (size_t i = 0; i < s->prof_used; i++) {
+        float t = 0.f;
+        ck(cudaEventElapsedTime(&t, s->prof_ev[2 * i], s->prof_ev[2 * i + 1]), "cudaEventElapsedTime");
+        if (kernel_ms) kernel_ms[s->prof_cls[i]] += t;
+        if (kernel_launches) kernel_launches[s->prof_cls[i]] += 1;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return s->check_status();
   });
 }
 

@@ -203,7 +203,7 @@ class Mesh:
             pass
 
 
-def make_params(config: Config, mesh: Mesh, keep_flux_balance: bool = False,
+def make_params(config: Config, mesh: Mesh, keep_stage_fields: bool = False,
                 patch_states: Optional[Sequence[Sequence[float]]] = None,
                 block_size: int = 0) -> "tuple[L.NfParams, object]":
     """nf_params for ``config`` on ``mesh`` (the patch array is returned too, to keep it alive)."""
@@ -215,7 +215,7 @@ def make_params(config: Config, mesh: Mesh, keep_flux_balance: bool = False,
     p.flux_scheme = L.NF_FLUX_RUSANOV
     p.precision = config.precision
     p.local_time_stepping = int(config.local_time_stepping)
-    p.keep_flux_balance = int(keep_flux_balance)
+    p.keep_stage_fields = int(keep_stage_fields)
     p.cfl = config.CFL
     p.t_end = config.t_end
     p.block_size = int(block_size)
@@ -264,10 +264,10 @@ class EulerSolver:
     """EulerSolver(config, grid): the device solver for one (possibly batched) mesh."""
 
     def __init__(self, config: Config, mesh: Mesh, U0: Optional[np.ndarray] = None,
-                 keep_flux_balance: bool = False, patch_states=None, block_size: int = 0):
+                 keep_stage_fields: bool = False, patch_states=None, block_size: int = 0):
         self.mesh = mesh
         self.n_cells = mesh.n_cells
-        params, self._patch_arr = make_params(config, mesh, keep_flux_balance, patch_states, block_size)
+        params, self._patch_arr = make_params(config, mesh, keep_stage_fields, patch_states, block_size)
         self._h = L.load().nf_create(mesh._h, C.byref(params))
         if not self._h:
             raise L.NetFluxError(L.NF_ERR_ARG, L.last_error(None))

@@ -1,0 +1,205 @@
+"""Parity of the CUDA path with the reference (golden fixtures) and the oracle.
+
+Tolerances are relative L-infinity errors per conserved variable, max over
+cells |a - b| / max |b| (the momentum components measured against the
+momentum magnitude max ||rho u||, see helpers.rel_linf):
+  * reference-order FP64: 1e-14 (bit-exact except pow() in far-field ghosts)
+  * FP64: 1e-12 after 1 TVD-RK3 step, 1e-9 after 100 steps
+  * mixed FP32 face work / FP64 state: 1e-5 after 1 step
+"""
+import numpy as np
+import pytest
+
+from helpers import CASES, config_for, golden, mesh, rel_l2, rel_linf
+from netflux_b200 import _lib as L
+from netflux_b200 import meshgen as mg
+from netflux_b200 import solver as S
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+TOL_REF = 1e-14
+TOL_FP64_1 = 1e-12
+TOL_FP64_100 = 1e-9
+TOL_MIXED_1 = 1e-5
+
+
+def run(g, precision, n_steps, time_scheme="TVD_RK3", spatial_order="Second", limiter="Barth", keep=False,
+        use_advance=False, **kw):
+    cfg = config_for(time_scheme=time_scheme, spatial_order=spatial_order, limiter=limiter, precision=precision,
+                     freestream=tuple(g["freestream"]), **kw)
+    m = mesh(g)
+    s = S.EulerSolver(cfg, m, U0=g["U0"], keep_stage_fields=keep)
+    dts = []
+    if use_advance:
+        s.advance(n_steps)
+    else:
+        for _ in range(n_steps):
+            s.calc_timestep(cfg)
+            dts.append(cfg.get_delta_time())
+            s.step(cfg)
+    U = s.get_solver_data().get_solution()
+    return s, U, np.array(dts)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_ref_order_one_step(case):
+    g = golden(case)
+    _, U, dts = run(g, "fp64_ref", 1)
+    assert rel_linf(dts, g["dt1"]) <= TOL_REF
+    assert rel_linf(U, g["U1"]) <= TOL_REF
+
+
+def test_ref_order_bitwise_without_far_field():
+    """No pow() on the path (slip walls only): the GPU reproduces the reference bit for bit."""
+    g = golden("slipbox5")
+    _, U, dts = run(g, "fp64_ref", 1)
+    assert np.array_equal(dts, g["dt1"])
+    assert np.array_equal(U, g["U1"])
+    _, U, dts = run(g, "fp64_ref", 100)
+    assert np.array_equal(U, g["U100"])
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_ref_order_stage_intermediates(case):
+    g = golden(case)
+    s, U, _ = run(g, "fp64_ref", 1, time_scheme="ExplicitEuler", keep=True)
+    d = s.get_solver_data()
+    nc = U.shape[0]
+    assert rel_linf(d.get_primvars(), g["euler_V"][:nc]) <= TOL_REF
+    assert rel_linf(d.get_primvars_gradient(), g["euler_grad"]) <= 1e-12
+    assert np.abs(d.get_primvars_limiter() - g["euler_limiter"]).max() <= 1e-12
+    assert rel_linf(d.get_flux_balance(), g["euler_R"]) <= 1e-12
+    assert rel_linf(U, g["euler_U"]) <= TOL_REF
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_fp64_one_and_hundred_steps(case):
+    g = golden(case)
+    _, U1, _ = run(g, "fp64", 1)
+    assert rel_linf(U1, g["U1"]) <= TOL_FP64_1
+    _, U100, _ = run(g, "fp64", 100, use_advance=True)
+    assert rel_linf(U100, g["U100"]) <= TOL_FP64_100
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_ref_order_hundred_steps(case):
+    g = golden(case)
+    _, U, _ = run(g, "fp64_ref", 100, use_advance=True)
+    assert rel_linf(U, g["U100"]) <= 1e-12
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_mixed_one_step(case):
+    g = golden(case)
+    _, U, _ = run(g, "mixed", 1)
+    err = rel_linf(U, g["U1"])
+    assert err <= TOL_MIXED_1, err
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_first_order(case):
+    g = golden(case)
+    _, U, dts = run(g, "fp64_ref", 3, spatial_order="First", limiter="NONE")
+    assert rel_linf(dts, g["first_dt3"]) <= TOL_REF
+    assert rel_linf(U, g["first_U3"]) <= TOL_REF
+
+
+def test_advance_graph_equals_step_loop():
+    g = golden("cube4")
+    _, a, _ = run(g, "fp64", 7)
+    _, b, _ = run(g, "fp64", 7, use_advance=True)
+    assert np.array_equal(a, b)
+
+
+def test_deterministic_repeat():
+    g = golden("sod40")
+    _, a, _ = run(g, "fp64", 20, use_advance=True)
+    _, b, _ = run(g, "fp64", 20, use_advance=True)
+    assert np.array_equal(a, b)
+
+
+def _oracle(g, n, **kw):
+    m = mesh(g)
+    pats = m.patches()
+    return po.run_oracle(m.export(), pats, [g["freestream"]] * len(pats), g["U0"], n, **kw)
+
+
+def test_local_time_stepping_matches_oracle():
+    g = golden("bump12")
+    _, U, _ = run(g, "fp64_ref", 10, local_time_stepping=True)
+    o = _oracle(g, 10, local_time_stepping=True, fields=False)
+    assert rel_linf(U, o["U"]) <= 1e-13
+
+
+def test_t_end_clipping_matches_oracle():
+    g = golden("sod40")
+    t_end = 0.9 * 5 * float(g["dt1"][0])
+    s, U, _ = run(g, "fp64_ref", 0, t_end=t_end)
+    time = s.advance(8)
+    o = _oracle(g, 8, t_end=t_end, fields=False)
+    assert abs(time - t_end) <= 1e-15 * t_end
+    assert rel_linf(U, g["U0"]) == 0.0  # the state before advancing
+    assert rel_linf(s.get_solver_data().get_solution(), o["U"]) <= 1e-13
+
+
+def test_residual_norms_match_oracle():
+    g = golden("cube4")
+    s, _, _ = run(g, "fp64", 3)
+    res = s.residual()
+    o = _oracle(g, 3, fields=False)
+    assert np.allclose(res[0], o["res"][-1], rtol=1e-12, atol=0)
+
+
+def test_batched_equals_individual_runs():
+    """Cases concatenated into one mesh advance exactly as they do alone (local dt)."""
+    gs = [golden("cube4"), golden("bump12")]
+    cfgs = [config_for(precision="fp64", local_time_stepping=True, freestream=tuple(g["freestream"])) for g in gs]
+    singles = []
+    for g, cfg in zip(gs, cfgs):
+        s = S.EulerSolver(cfg, mesh(g), U0=g["U0"])
+        s.advance(5)
+        singles.append(s.get_solver_data().get_solution())
+    ms = [mesh(g) for g in gs]
+    batch = S.Mesh.concat(ms)
+    states = [list(g["freestream"]) for g, m in zip(gs, ms) for _ in m.patches()]
+    sb = S.EulerSolver(cfgs[0], batch, U0=np.concatenate([g["U0"] for g in gs]), patch_states=states)
+    sb.advance(5)
+    Ub = sb.get_solver_data().get_solution()
+    off = batch.case_offsets()
+    for k, U in enumerate(singles):
+        assert np.array_equal(Ub[off[k]:off[k + 1]], U)
+    r = sb.residual()
+    assert r.shape == (2, 2) and np.all(r[:, 0] > 0)
+
+
+def test_nonphysical_state_is_reported():
+    """A negative pressure injected on the host surfaces as an error status, not a fault."""
+    g = golden("cube4")
+    U0 = g["U0"].copy()
+    U0[17, 4] = -1.0  # negative total energy -> negative pressure
+    cfg = config_for(precision="fp64", freestream=tuple(g["freestream"]))
+    s = S.EulerSolver(cfg, mesh(g), U0=U0)
+    with pytest.raises((L.NetFluxError, RuntimeError)):
+        s.calc_timestep(cfg)
+        s.step(cfg)
+        s.synchronize()
+
+
+def test_sod_tube_against_oracle_and_mixed_error():
+    """Sod tube with the limiter active at the shock: FP64 and mixed vs the oracle."""
+    m = mg.sod_mesh(100, 4, 4, jitter=0.05, seed=5)
+    U0 = mg.sod_initial_state(m)
+    mm = S.Mesh.from_tet_mesh(m)
+    pats = mm.patches()
+    n = 60
+    o = po.run_oracle(mm.export(), pats, [mg.SOD_LEFT] * len(pats), U0, n, fields=False)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        cfg = config_for(precision=prec, freestream=mg.SOD_LEFT)
+        s = S.EulerSolver(cfg, mm, U0=U0)
+        s.advance(n)
+        out[prec] = s.get_solver_data().get_solution()
+    assert rel_linf(out["fp64"], o["U"]) <= TOL_FP64_100
+    assert rel_linf(out["mixed"], o["U"]) <= 1e-3
+    assert rel_l2(out["mixed"], o["U"]) <= 1e-4
