@@ -202,6 +202,20 @@ int nf_time_steps(nf_solver* s, int64_t n_steps, int per_kernel, double* ms_tota
 const char* nf_last_error(const nf_solver* s);
 void nf_destroy(nf_solver* s);
 
+/* Residual norms without any device allocation: out[0] = sqrt(sum v^2 / n),
+ * out[1] = max |v| over the n doubles at the device pointer `values`; `out`
+ * is a device pointer to 2 doubles; work is queued on `stream` (a
+ * cudaStream_t, NULL for the default stream) and is complete when the stream
+ * reaches it. For callers that cannot allocate device memory when they need
+ * the reduction (inside CUDA graph capture, under a fixed memory pool, in a
+ * real-time loop). Its per-block partial sums live in a fixed 128 KiB array
+ * in the library, so n is limited to 134,217,728; larger n returns
+ * NF_ERR_ARG. The first call on a device looks up that array's address and
+ * should come before any stream capture; calls that overlap on the GPU share
+ * the array and race. It has no counterpart in the reference, which computes
+ * no residual norms. */
+int nf_residual_norms_noalloc(const double* values, int64_t n, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -144,6 +144,11 @@ __global__ void gather_state_kernel(int n, int st, const long long* __restrict__
 
 }  // namespace
 
+namespace nf {
+// Error text returned by nf_last_error(NULL) for calls that have no solver.
+void set_last_error_text(const std::string& msg) { g_create_error = msg; }
+}  // namespace nf
+
 struct nf_solver {
   int device = 0;
   cudaStream_t stream = nullptr;
