@@ -261,9 +261,11 @@ def main():
     lib = L.load()
     N = mesh.n_cells
 
-    # warm-up (also builds the CUDA graph of the step)
+    # warm-up, launch-shape tuning, then the CUDA graph of the step
     ms = C.c_double()
-    solver.advance(max(args.warmup, 3))
+    solver.advance(max(args.warmup, 3) - 1)
+    tuned = solver.tune() if args.block == 0 else None
+    solver.advance(1)
     kms = (C.c_double * L.NF_KERNEL_COUNT)()
     kl = (C.c_int64 * L.NF_KERNEL_COUNT)()
     if dist:
@@ -343,7 +345,8 @@ def main():
             "config": {"workload": desc, "cells": N, "faces": mesh.n_faces, "time_scheme": "TVD_RK3",
                        "local_time_stepping": lts, "cfl": 0.8, "precision": args.precision,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "working set > 126 MB L2 (no flush needed)", "mesh_build_s": round(t_mesh, 2)},
+                       "l2": "working set > 126 MB L2 (no flush needed)", "mesh_build_s": round(t_mesh, 2),
+                       "launch_shapes": tuned},
             "roofline": roof,
             "step_roofline": {"model_bytes_per_cell_stage": round(model, 1), "achieved": round(step_gbs, 1),
                               "peak": hbm, "unit": "GB/s", "frac": round(step_gbs / hbm, 4)},

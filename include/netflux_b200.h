@@ -183,6 +183,14 @@ int nf_get_field(nf_solver* s, int which, double* out, int64_t n_values);
 /* Wait for queued work; report a device-side validity failure. */
 int nf_synchronize(nf_solver* s);
 
+/* Time the launch shapes of the gradient and flux kernels on the current
+ * state and keep the fastest: block size (64 or 128 threads) and whether each
+ * thread issues its next variable's / face's loads before the current
+ * arithmetic. config (may be NULL) receives {gradient block, gradient
+ * variant, flux block, flux variant}. The state is unchanged. The reference
+ * has no counterpart (it runs on one CPU thread). */
+int nf_tune(nf_solver* s, int* config);
+
 /* Kernel classes reported by nf_time_steps. */
 #define NF_KERNEL_TIMESTEP 0
 #define NF_KERNEL_GRADIENT 1

@@ -30,7 +30,7 @@ EXPORTED = (
     "nf_mesh_export", "nf_mesh_get_permutation", "nf_mesh_get_case_offsets", "nf_mesh_destroy",
     "nf_params_default", "nf_create", "nf_set_state", "nf_get_state", "nf_calc_timestep", "nf_set_timestep",
     "nf_step", "nf_advance", "nf_get_residual", "nf_get_field", "nf_synchronize", "nf_last_error", "nf_destroy",
-    "nf_time_steps", "nf_residual_norms_noalloc",
+    "nf_time_steps", "nf_residual_norms_noalloc", "nf_tune",
 )
 NF_KERNEL_TIMESTEP, NF_KERNEL_GRADIENT, NF_KERNEL_FLUX, NF_KERNEL_OTHER, NF_KERNEL_COUNT = range(5)
 
@@ -99,6 +99,7 @@ def load() -> C.CDLL:
         "nf_destroy": (None, [P]),
         "nf_time_steps": (I, [P, I64, I, dp, dp, i64p]),
         "nf_residual_norms_noalloc": (I, [P, I64, P, P]),
+        "nf_tune": (I, [P, C.POINTER(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -17,10 +17,15 @@
 //   face states fs : [4][5][stride], the limited reconstruction of the cell's
 //               primitives at each of its faces (written by the gradient
 //               kernel, read by the flux kernel of both adjacent cells)
-//   face SoA    S, nhat, ri, rj : [3][F]; area : [F]
+//   face SoA    S, nhat : [3][F]; area : [F]
+//   slot SoA    rs : [3][4][stride], the vector from the cell centroid to the
+//               centroid of each of its faces (r_i or r_j of the face)
+//   boundary    b_cell, b_slot, b_face, b_patch : [nb]; ghost states vg and
+//               boundary fluxes fb : [5][bstride]
 // Each face's flux is evaluated by both of its cells with the owner on the
 // left, so both see bit-identical values; no atomics, deterministic results.
-// The gradient and flux kernels run four threads per cell (one per face slot).
+// The gradient kernel runs one thread per (cell, variable), the flux kernel
+// four threads per cell (one per face slot).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -37,15 +42,24 @@ struct MeshView {
   int stride;     // SoA stride of cell arrays
   int n_faces;
   const int* __restrict__ slot;    // [4][stride] face << 1 | side
-  const int* __restrict__ nbslot;  // [4][stride] neighbour << 2 | its slot, or -(1 + patch)
-  const T* __restrict__ S;
-  const T* __restrict__ nhat;
-  const T* __restrict__ area;
-  const T* __restrict__ ri;
-  const T* __restrict__ rj;
+  const int* __restrict__ nbslot;  // [4][stride] neighbour << 2 | its slot, or -(1 + boundary face)
+  const T* __restrict__ S;         // [3][F]
+  const T* __restrict__ nhat;      // [3][F]
+  const T* __restrict__ area;      // [F]
+  const T* __restrict__ rs;        // [3][4][stride] centroid-to-face vector of each slot
+  const T* __restrict__ sg;        // [3][4][stride] face normal seen from the cell (outward), 0 for no face
+  const int* __restrict__ nbv;     // [4][stride] neighbour cell, -(1 + boundary face), or the cell itself for no face
+  const T* __restrict__ hvinv;     // [stride] 0.5 / vol
   const double* __restrict__ vol;
   const double* __restrict__ dS;
   const PatchBC* __restrict__ patches;
+  // boundary faces, ordered by owner cell
+  int nb;                          // number of boundary faces
+  int bstride;                     // SoA stride of boundary arrays
+  const int* __restrict__ b_cell;  // owner cell
+  const int* __restrict__ b_slot;  // owner's slot of the face
+  const int* __restrict__ b_face;  // face id (geometry)
+  const int* __restrict__ b_patch; // patch
 };
 
 struct StageArgs {
@@ -73,6 +87,11 @@ struct StageArgs {
   float* fs32;
   float* grad32;
   float* phi32;
+  // boundary faces: cell-centre ghost states [5][bstride] and boundary fluxes [5][bstride]
+  double* vg;
+  double* fb;
+  float* vg32;
+  float* fb32;
 };
 
 enum : int { kScalDtMin = 0, kScalTime = 1, kScalTEnd = 2, kScalDtUsed = 3, kScalCount = 8 };
@@ -135,157 +154,116 @@ __device__ __forceinline__ T quad_max_tree(T v) {
 }
 
 // ---------------------------------------------------------------------------
-// Green-Gauss gradient + min/max + Barth limiter of one cell
+// Green-Gauss gradient + min/max + Barth limiter
 // (calc_green_gauss_gradient, calc_max_and_min_values, calc_barth_limiter,
-//  Numerics.hpp:86-292), then the limited reconstruction at each of its faces
+//  Numerics.hpp:86-292), then the limited reconstruction at each face
 // (calc_limited_reconstruction, Numerics.hpp:135-145), which is what the flux
 // kernel consumes. Ghost states at boundary faces are the cell-centre ghosts
 // of set_constant_ghost_values (Solver.cpp:300-330).
+//
+// One thread per (cell, primitive variable k): every step of this kernel acts
+// on one variable at a time, so the five threads of a cell share nothing but
+// the cell's geometry (same addresses, served once per warp). Each thread
+// folds its cell's faces in slot order, exactly as the reference's face loops
+// reach that cell.
 // ---------------------------------------------------------------------------
 template <typename T, bool kRef>
 __global__ void __launch_bounds__(256) gradient_limiter_kernel(MeshView<T> m, StageArgs a) {
-  const int q = threadIdx.x & 3;
-  int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
-  const bool valid = c < m.n;
-  if (!valid) c = m.n - 1;  // every lane takes part in the quad shuffles
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = t / 5;
+  const int k = t - 5 * c;
+  if (c >= m.n) return;
   const int st = m.stride;
   const int F = m.n_faces;
-  T Vc[5];
+  int sl[4], ns[4];
 #pragma unroll
-  for (int k = 0; k < 5; k++) Vc[k] = ld_v<T>(a, k * st + c);
-  const T vol = T(m.vol[c]);
-  const int sl = m.slot[q * st + c];
-  const int ns = m.nbslot[q * st + c];
-  const bool has = sl >= 0;
-  const int f = has ? (sl >> 1) : 0;
-  const bool own = (sl & 1) == 0;
-
-  // this face's Green-Gauss term (reference: already divided by the volume)
-  // and its max/min candidates
-  T t[5][3], mx[5], mn[5];
-  if (has) {
-    const T S[3] = {m.S[f], m.S[F + f], m.S[2 * F + f]};
-    // the neighbour side of a face subtracts its term: (-x)/v == -(x/v) and
-    // g + (-y) == g - y exactly, so a signed normal reproduces both branches
-    const T Sg[3] = {own ? S[0] : -S[0], own ? S[1] : -S[1], own ? S[2] : -S[2]};
-    T Vo[5];
-    if (ns >= 0) {
-      const int o = ns >> 2;
-#pragma unroll
-      for (int k = 0; k < 5; k++) Vo[k] = ld_v<T>(a, k * st + o);
-    } else {
-      const T nh[3] = {m.nhat[f], m.nhat[F + f], m.nhat[2 * F + f]};
-      ghost_state<T>(m.patches[-ns - 1], Vc, nh, Vo);
-    }
-#pragma unroll
-    for (int k = 0; k < 5; k++) {
-      const T uf = T(0.5) * (Vc[k] + Vo[k]);  // 0.5 (V_i + V_j); the sum commutes
-#pragma unroll
-      for (int d = 0; d < 3; d++) {
-        if constexpr (kRef) t[k][d] = uf * Sg[d] / vol;
-        else t[k][d] = uf * Sg[d];
-      }
-      if constexpr (kRef) {
-        const T vi = own ? Vc[k] : Vo[k], vj = own ? Vo[k] : Vc[k];
-        mx[k] = rmax(vi, vj);
-        mn[k] = rmin(vi, vj);
-      } else {
-        mx[k] = Vo[k];
-        mn[k] = Vo[k];
-      }
-    }
-  } else {
-#pragma unroll
-    for (int k = 0; k < 5; k++) {
-      t[k][0] = t[k][1] = t[k][2] = T(-0.0);
-      mx[k] = -std::numeric_limits<T>::max();
-      mn[k] = std::numeric_limits<T>::max();
-    }
+  for (int q = 0; q < 4; q++) {
+    sl[q] = m.slot[q * st + c];
+    ns[q] = m.nbslot[q * st + c];
   }
-  // gradient of the cell: sum of the quad's terms
-  T g[5][3];
-  T vmax[5], vmin[5];
+  const T vc = ld_v<T>(a, k * st + c);
+  const T vol = T(m.vol[c]);
+  T g[3] = {T(0), T(0), T(0)};
+  T vmax = -std::numeric_limits<T>::max(), vmin = std::numeric_limits<T>::max();
 #pragma unroll
-  for (int k = 0; k < 5; k++) {
+  for (int q = 0; q < 4; q++) {
+    if (sl[q] < 0) continue;
+    const int f = sl[q] >> 1;
+    const bool own = (sl[q] & 1) == 0;
+    T vo;
+    if (ns[q] >= 0) vo = ld_v<T>(a, k * st + (ns[q] >> 2));
+    else if constexpr (sizeof(T) == 8) vo = a.vg[k * m.bstride + (-ns[q] - 1)];
+    else vo = a.vg32[k * m.bstride + (-ns[q] - 1)];
+    // the neighbour side subtracts its term: (-x)/v == -(x/v) and
+    // g + (-y) == g - y exactly, so a signed normal reproduces both branches
+    const T s0 = m.S[f], s1 = m.S[F + f], s2 = m.S[2 * F + f];
+    const T Sg[3] = {own ? s0 : -s0, own ? s1 : -s1, own ? s2 : -s2};
+    const T uf = T(0.5) * (vc + vo);  // 0.5 (V_i + V_j); the sum commutes exactly
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-      if constexpr (kRef) g[k][d] = quad_sum_ordered(t[k][d]);
-      else g[k][d] = quad_sum_tree(t[k][d]);
+      if constexpr (kRef) g[d] = g[d] + uf * Sg[d] / vol;
+      else g[d] = fma(uf, Sg[d], g[d]);
     }
     if constexpr (kRef) {
-      vmax[k] = quad_max_ordered(-std::numeric_limits<T>::max(), mx[k]);
-      vmin[k] = quad_min_ordered(std::numeric_limits<T>::max(), mn[k]);
+      const T vi = own ? vc : vo, vj = own ? vo : vc;  // max(V_i, V_j) in the face's operand order
+      vmax = rmax(vmax, rmax(vi, vj));
+      vmin = rmin(vmin, rmin(vi, vj));
     } else {
-      vmax[k] = fmax(Vc[k], quad_max_tree(mx[k]));
-      vmin[k] = fmin(Vc[k], quad_min_tree(mn[k]));
+      vmax = fmax(vmax, vo);
+      vmin = fmin(vmin, vo);
     }
   }
   if constexpr (!kRef) {
     const T iv = T(1) / vol;
-#pragma unroll
-    for (int k = 0; k < 5; k++)
-#pragma unroll
-      for (int d = 0; d < 3; d++) g[k][d] *= iv;
+    g[0] *= iv;
+    g[1] *= iv;
+    g[2] *= iv;
+    vmax = fmax(vmax, vc);
+    vmin = fmin(vmin, vc);
   }
-  // grad V . r at this lane's face: the limiter's Delta_2 before its
-  // sign/epsilon adjustment, and the increment of the reconstruction
-  T gr[5];
-  {
-    const T* rr = own ? m.ri : m.rj;
-    const T r[3] = {rr[f], rr[F + f], rr[2 * F + f]};
+  // grad V_k . r at each face: the limiter's Delta_2 before its sign/epsilon
+  // adjustment, and the increment of the reconstruction
+  T gr[4];
 #pragma unroll
-    for (int k = 0; k < 5; k++) gr[k] = (g[k][0] * r[0] + g[k][1] * r[1]) + g[k][2] * r[2];
+  for (int q = 0; q < 4; q++) {
+    const T* r = m.rs + q * st + c;  // [d][q][cell]
+    gr[q] = (g[0] * r[0] + g[1] * r[4 * st]) + g[2] * r[8 * st];
   }
-  T phi[5];
+  T phi = T(1);
   if (a.barth) {
+    phi = std::numeric_limits<T>::max();
 #pragma unroll
-    for (int k = 0; k < 5; k++) {
-      T fc = std::numeric_limits<T>::max();  // identity of the min for an empty slot
-      if (has) {
-        T d2 = gr[k];
-        const T sg = (d2 > T(0)) ? T(1) : ((d2 < T(0)) ? T(-1) : T(0));
-        d2 = sg * (fabs(d2) + Gas<T>::eps);
-        if (d2 != T(0)) {
-          const T num = (d2 > T(0)) ? vmax[k] - Vc[k] : vmin[k] - Vc[k];
-          fc = rmin(T(1), num / d2);
-        } else {
-          fc = T(1);
-        }
+    for (int q = 0; q < 4; q++) {
+      if (sl[q] < 0) continue;
+      T d2 = gr[q];
+      const T sg = (d2 > T(0)) ? T(1) : ((d2 < T(0)) ? T(-1) : T(0));
+      d2 = sg * (fabs(d2) + Gas<T>::eps);
+      T fc = T(1);
+      if (d2 != T(0)) {
+        const T num = (d2 > T(0)) ? vmax - vc : vmin - vc;
+        fc = rmin(T(1), num / d2);
       }
-      if constexpr (kRef) phi[k] = quad_min_ordered(std::numeric_limits<T>::max(), fc);
-      else phi[k] = quad_min_tree(fc);
+      phi = rmin(phi, fc);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    if (sl[q] < 0) continue;
+    const T v = vc + phi * gr[q];
+    if constexpr (sizeof(T) == 8) a.fs[(q * 5 + k) * st + c] = v;
+    else a.fs32[(q * 5 + k) * st + c] = v;
+  }
+  if constexpr (sizeof(T) == 8) {
+    if (a.grad) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) a.grad[(k * 3 + d) * st + c] = g[d];
+      a.phi[k * st + c] = phi;
     }
   } else {
+    if (a.grad32) {
 #pragma unroll
-    for (int k = 0; k < 5; k++) phi[k] = T(1);
-  }
-  if (valid && has) {
-#pragma unroll
-    for (int k = 0; k < 5; k++) {
-      const T v = Vc[k] + phi[k] * gr[k];
-      if constexpr (sizeof(T) == 8) a.fs[(q * 5 + k) * st + c] = v;
-      else a.fs32[(q * 5 + k) * st + c] = v;
-    }
-  }
-  if (valid && q == 0) {
-    if constexpr (sizeof(T) == 8) {
-      if (a.grad) {
-#pragma unroll
-        for (int k = 0; k < 5; k++) {
-#pragma unroll
-          for (int d = 0; d < 3; d++) a.grad[(k * 3 + d) * st + c] = g[k][d];
-          a.phi[k * st + c] = phi[k];
-        }
-      }
-    } else {
-      if (a.grad32) {
-#pragma unroll
-        for (int k = 0; k < 5; k++) {
-#pragma unroll
-          for (int d = 0; d < 3; d++) a.grad32[(k * 3 + d) * st + c] = g[k][d];
-          a.phi32[k * st + c] = phi[k];
-        }
-      }
+      for (int d = 0; d < 3; d++) a.grad32[(k * 3 + d) * st + c] = g[d];
+      a.phi32[k * st + c] = phi;
     }
   }
 }
@@ -313,35 +291,34 @@ __global__ void __launch_bounds__(256) flux_update_kernel(MeshView<T> m, StageAr
   const bool own = (sl & 1) == 0;
   // this face's contribution to R: -F on the owner side, +F on the other
   double contrib[5] = {-0.0, -0.0, -0.0, -0.0, -0.0};
-  if (has) {
+  if (has && ns < 0) {
+    // boundary face (this cell is its owner): flux from boundary_flux_kernel
+    const int b = -ns - 1;
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      if constexpr (sizeof(T) == 8) contrib[k] = -a.fb[k * m.bstride + b];
+      else contrib[k] = -double(a.fb32[k * m.bstride + b]);
+    }
+  } else if (has) {
     const int f = sl >> 1;
     const T nh[3] = {m.nhat[f], m.nhat[F + f], m.nhat[2 * F + f]};
     const T area = m.area[f];
     T Vs[5], Vx[5];  // this cell's face state, the other side's
+    const int o = ns >> 2, q2 = ns & 3;
 #pragma unroll
     for (int k = 0; k < 5; k++) {
       if (second) {
-        if constexpr (sizeof(T) == 8) Vs[k] = a.fs[(q * 5 + k) * st + c];
-        else Vs[k] = a.fs32[(q * 5 + k) * st + c];
+        if constexpr (sizeof(T) == 8) {
+          Vs[k] = a.fs[(q * 5 + k) * st + c];
+          Vx[k] = a.fs[(q2 * 5 + k) * st + o];
+        } else {
+          Vs[k] = a.fs32[(q * 5 + k) * st + c];
+          Vx[k] = a.fs32[(q2 * 5 + k) * st + o];
+        }
       } else {
         Vs[k] = ld_v<T>(a, k * st + c);
+        Vx[k] = ld_v<T>(a, k * st + o);
       }
-    }
-    if (ns >= 0) {
-      const int o = ns >> 2, q2 = ns & 3;
-#pragma unroll
-      for (int k = 0; k < 5; k++) {
-        if (second) {
-          if constexpr (sizeof(T) == 8) Vx[k] = a.fs[(q2 * 5 + k) * st + o];
-          else Vx[k] = a.fs32[(q2 * 5 + k) * st + o];
-        } else {
-          Vx[k] = ld_v<T>(a, k * st + o);
-        }
-      }
-    } else {
-      // boundary face (this cell is its owner): ghost from the reconstructed
-      // face value (Solver.cpp:212)
-      ghost_state<T>(m.patches[-ns - 1], Vs, nh, Vx);
     }
     const T* VL = own ? Vs : Vx;
     const T* VR = own ? Vx : Vs;
@@ -360,7 +337,10 @@ __global__ void __launch_bounds__(256) flux_update_kernel(MeshView<T> m, StageAr
   // flux balance, accumulated in face-slot order: ((0 + c0) + c1) + ...
   double R[5];
 #pragma unroll
-  for (int k = 0; k < 5; k++) R[k] = quad_sum_ordered(contrib[k]);
+  for (int k = 0; k < 5; k++) {
+    if constexpr (kRef) R[k] = quad_sum_ordered(contrib[k]);
+    else R[k] = quad_sum_tree(contrib[k]);
+  }
 
   // ---- stage update (FP64); every lane computes it, lanes store by component ----
   const double vol = m.vol[c];
@@ -405,6 +385,294 @@ __global__ void __launch_bounds__(256) flux_update_kernel(MeshView<T> m, StageAr
     for (int k = 0; k < 5; k++) finite = finite && isfinite(R[k]) && isfinite(Unew[k]);
     if (!finite) atomicOr(a.status, kErrNonFinite);
     else if (!(Vn[0] > 0.0) || !(Vn[4] > 0.0)) atomicOr(a.status, kErrNonPhysical);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fast forms (FP64 with contraction, and mixed FP32): one thread per cell.
+//
+// gradient_fast_kernel: the same Green-Gauss gradient, min/max, Barth limiter
+// and reconstruction, rearranged for fewer instructions (results agree with
+// the reference form to round-off):
+//   grad V = 0.5/vol (sum_q V_q S_q + V_c sum_q S_q) with S_q the outward
+//   normal of slot q; a missing slot has S_q = 0, r_q = 0 and points at the
+//   cell itself, so it changes nothing and needs no branch;
+//   phi = min(1, min_q A_q / D_q) with A_q = (V_max - V_c) or (V_c - V_min)
+//   and D_q = |grad V . r_q| + eps: the minimising face is found by
+//   cross-multiplication, then one division per variable.
+// ---------------------------------------------------------------------------
+template <typename T, bool kPipe>
+__global__ void __launch_bounds__(128) gradient_fast_kernel(MeshView<T> m, StageArgs a) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.n) return;
+  const int st = m.stride;
+  const T* Vin = nullptr;
+  const T* Vg = nullptr;
+  T* fs = nullptr;
+  if constexpr (sizeof(T) == 8) {
+    Vin = reinterpret_cast<const T*>(a.Vin);
+    Vg = reinterpret_cast<const T*>(a.vg);
+    fs = reinterpret_cast<T*>(a.fs);
+  } else {
+    Vin = reinterpret_cast<const T*>(a.Vin32);
+    Vg = reinterpret_cast<const T*>(a.vg32);
+    fs = reinterpret_cast<T*>(a.fs32);
+  }
+  int nb[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) nb[q] = m.nbv[q * st + c];
+  // the values of variable k: own and the four neighbours (or ghosts)
+  auto fetch = [&](int k, T& vc, T vo[4]) {
+    const T* Vk = Vin + k * st;
+    vc = Vk[c];
+#pragma unroll
+    for (int q = 0; q < 4; q++) vo[q] = nb[q] >= 0 ? Vk[nb[q]] : Vg[k * m.bstride + (-nb[q] - 1)];
+  };
+  T vcN, voN[4];
+  if (kPipe) fetch(0, vcN, voN);
+  T sgv[4][3];
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int d = 0; d < 3; d++) sgv[q][d] = m.sg[(d * 4 + q) * st + c];
+  const T ssum[3] = {(sgv[0][0] + sgv[1][0]) + (sgv[2][0] + sgv[3][0]),
+                     (sgv[0][1] + sgv[1][1]) + (sgv[2][1] + sgv[3][1]),
+                     (sgv[0][2] + sgv[1][2]) + (sgv[2][2] + sgv[3][2])};
+  const T hv = m.hvinv[c];
+#pragma unroll 1
+  for (int k = 0; k < 5; k++) {
+    T vc, vo[4];
+    if (kPipe) {
+      vc = vcN;
+#pragma unroll
+      for (int q = 0; q < 4; q++) vo[q] = voN[q];
+      if (k < 4) fetch(k + 1, vcN, voN);  // next variable's loads overlap this one's arithmetic
+    } else {
+      fetch(k, vc, vo);
+    }
+    T acc[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      acc[d] = vc * ssum[d];
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[d] = fma(vo[q], sgv[q][d], acc[d]);
+    }
+    const T g[3] = {hv * acc[0], hv * acc[1], hv * acc[2]};
+    const T vmax = fmax(fmax(fmax(vc, vo[0]), fmax(vo[1], vo[2])), vo[3]);
+    const T vmin = fmin(fmin(fmin(vc, vo[0]), fmin(vo[1], vo[2])), vo[3]);
+    T gr[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const T* r = m.rs + q * st + c;
+      gr[q] = fma(g[2], r[8 * st], fma(g[1], r[4 * st], g[0] * r[0]));
+    }
+    T phi = T(1);
+    if (a.barth) {
+      T An = T(1), Dn = T(1);  // best ratio so far, starting at 1
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const T d2 = gr[q];
+        const T A = d2 > T(0) ? vmax - vc : vc - vmin;
+        const T D = fabs(d2) + Gas<T>::eps;
+        const bool better = (d2 != T(0)) && (A * Dn < An * D);
+        An = better ? A : An;
+        Dn = better ? D : Dn;
+      }
+      phi = An / Dn;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) fs[(q * 5 + k) * st + c] = fma(phi, gr[q], vc);
+    if constexpr (sizeof(T) == 8) {
+      if (a.grad) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) a.grad[(k * 3 + d) * st + c] = g[d];
+        a.phi[k * st + c] = phi;
+      }
+    } else {
+      if (a.grad32) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) a.grad32[(k * 3 + d) * st + c] = g[d];
+        a.phi32[k * st + c] = phi;
+      }
+    }
+  }
+}
+
+// flux_fast_kernel: the flux balance and stage update of one cell per thread.
+// Interior faces use the two face states; boundary faces add the flux that
+// boundary_flux_kernel computed. The next face's loads are issued before the
+// current face's flux is evaluated.
+template <typename T>
+struct FaceInput {
+  T s[5];      // this cell's face state, or the boundary flux
+  T x[5];      // the other side's face state
+  T n[3];
+  T area;
+  int kind;    // 0 no face, 1 interior (owner), 2 interior (neighbour side), 3 boundary
+};
+
+template <typename T, bool kPipe>
+__global__ void __launch_bounds__(128) flux_fast_kernel(MeshView<T> m, StageArgs a) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.n) return;
+  const int st = m.stride;
+  const int F = m.n_faces;
+  const bool second = a.second_order != 0;
+  const T* fsb = nullptr;
+  const T* Vin = nullptr;
+  const T* fb = nullptr;
+  if constexpr (sizeof(T) == 8) {
+    fsb = reinterpret_cast<const T*>(a.fs);
+    Vin = reinterpret_cast<const T*>(a.Vin);
+    fb = reinterpret_cast<const T*>(a.fb);
+  } else {
+    fsb = reinterpret_cast<const T*>(a.fs32);
+    Vin = reinterpret_cast<const T*>(a.Vin32);
+    fb = reinterpret_cast<const T*>(a.fb32);
+  }
+  int sl[4], ns[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    sl[q] = m.slot[q * st + c];
+    ns[q] = m.nbslot[q * st + c];
+  }
+  auto fetch = [&](int q, FaceInput<T>& in) {
+    const int s_ = sl[q], n_ = ns[q];
+    if (s_ < 0) {
+      in.kind = 0;
+    } else if (n_ < 0) {
+      in.kind = 3;
+      const int b = -n_ - 1;
+#pragma unroll
+      for (int k = 0; k < 5; k++) in.s[k] = fb[k * m.bstride + b];
+    } else {
+      const int f = s_ >> 1, o = n_ >> 2, q2 = n_ & 3;
+      in.kind = (s_ & 1) ? 2 : 1;
+#pragma unroll
+      for (int k = 0; k < 5; k++) {
+        in.s[k] = second ? fsb[(q * 5 + k) * st + c] : Vin[k * st + c];
+        in.x[k] = second ? fsb[(q2 * 5 + k) * st + o] : Vin[k * st + o];
+      }
+      in.n[0] = m.nhat[f];
+      in.n[1] = m.nhat[F + f];
+      in.n[2] = m.nhat[2 * F + f];
+      in.area = m.area[f];
+    }
+  };
+  double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  FaceInput<T> nxt;
+  if (kPipe) fetch(0, nxt);
+#pragma unroll 1
+  for (int q = 0; q < 4; q++) {
+    FaceInput<T> cur;
+    if (kPipe) {
+      cur = nxt;
+      if (q < 3) fetch(q + 1, nxt);  // next face's loads overlap this face's flux
+    } else {
+      fetch(q, cur);
+    }
+    if (cur.kind == 3) {
+#pragma unroll
+      for (int k = 0; k < 5; k++) R[k] -= double(cur.s[k]);
+    } else if (cur.kind != 0) {
+      const bool own = cur.kind == 1;
+      T Fl[5];
+      if (own) rusanov_fast<T>(cur.s, cur.x, cur.n, cur.area, Fl);
+      else rusanov_fast<T>(cur.x, cur.s, cur.n, cur.area, Fl);
+#pragma unroll
+      for (int k = 0; k < 5; k++) R[k] = own ? R[k] - double(Fl[k]) : R[k] + double(Fl[k]);
+    }
+  }
+  const double vol = m.vol[c];
+  const double dt = a.local_dt ? a.dt_local[c] : stage_dt(a.scal);
+  double Unew[5];
+  if (a.scheme == 0 || a.stage == 0) {
+    const double qf = dt / vol;
+#pragma unroll
+    for (int k = 0; k < 5; k++) Unew[k] = fma(qf, R[k], a.Uin[k * st + c]);
+  } else if (a.stage == 1) {
+    const double qf = 0.25 * dt / vol;
+#pragma unroll
+    for (int k = 0; k < 5; k++) Unew[k] = 0.75 * a.Un[k * st + c] + 0.25 * a.Uin[k * st + c] + qf * R[k];
+  } else {
+    const double qf = 2.0 / 3.0 * dt / vol;
+#pragma unroll
+    for (int k = 0; k < 5; k++) Unew[k] = 1.0 / 3.0 * a.Un[k * st + c] + 2.0 / 3.0 * a.Uin[k * st + c] + qf * R[k];
+  }
+  double Vn[5];
+  cons_to_prim<double, false>(Unew, Vn);
+  bool finite = true;
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    a.Uout[k * st + c] = Unew[k];
+    a.Vout[k * st + c] = Vn[k];
+    if (a.Vout32) a.Vout32[k * st + c] = float(Vn[k]);
+    if (a.R) a.R[k * st + c] = R[k];
+    finite = finite && isfinite(R[k]) && isfinite(Unew[k]);
+  }
+  if (a.res_cell) a.res_cell[c] = R[0] / vol;
+  if (!finite) atomicOr(a.status, kErrNonFinite);
+  else if (!(Vn[0] > 0.0) || !(Vn[4] > 0.0)) atomicOr(a.status, kErrNonPhysical);
+}
+
+// ---------------------------------------------------------------------------
+// Boundary faces. ghost_kernel: the cell-centre ghost state of every boundary
+// face (set_constant_ghost_values, Solver.cpp:300-330), read by the gradient
+// kernel like a neighbour's primitives. boundary_flux_kernel: the flux through
+// every boundary face, from the owner's reconstructed face state and the ghost
+// built from that state (Solver.cpp:197-229), read by the flux kernel at the
+// face's slot. One thread per boundary face; the hot kernels carry no
+// boundary-condition code.
+// ---------------------------------------------------------------------------
+template <typename T, bool kRef>
+__global__ void __launch_bounds__(256) ghost_kernel(MeshView<T> m, StageArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= m.nb) return;
+  const int c = m.b_cell[b], f = m.b_face[b];
+  const int F = m.n_faces, st = m.stride;
+  T V[5], G[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) V[k] = ld_v<T>(a, k * st + c);
+  const T nh[3] = {m.nhat[f], m.nhat[F + f], m.nhat[2 * F + f]};
+  ghost_state<T>(m.patches[m.b_patch[b]], V, nh, G);
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    if constexpr (sizeof(T) == 8) a.vg[k * m.bstride + b] = G[k];
+    else a.vg32[k * m.bstride + b] = G[k];
+  }
+}
+
+template <typename T, bool kRef>
+__global__ void __launch_bounds__(256) boundary_flux_kernel(MeshView<T> m, StageArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= m.nb) return;
+  const int c = m.b_cell[b], q = m.b_slot[b], f = m.b_face[b];
+  const int F = m.n_faces, st = m.stride;
+  T VL[5], VR[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    if (a.second_order) {
+      if constexpr (sizeof(T) == 8) VL[k] = a.fs[(q * 5 + k) * st + c];
+      else VL[k] = a.fs32[(q * 5 + k) * st + c];
+    } else {
+      VL[k] = ld_v<T>(a, k * st + c);
+    }
+  }
+  const T nh[3] = {m.nhat[f], m.nhat[F + f], m.nhat[2 * F + f]};
+  ghost_state<T>(m.patches[m.b_patch[b]], VL, nh, VR);
+  T Fl[5];
+  if constexpr (kRef) {
+    T UL[5], UR[5];
+    prim_to_cons<T, kRef>(VL, UL);
+    prim_to_cons<T, kRef>(VR, UR);
+    rusanov_ref<T>(UL, UR, nh, m.area[f], Fl);
+  } else {
+    rusanov_fast<T>(VL, VR, nh, m.area[f], Fl);
+  }
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    if constexpr (sizeof(T) == 8) a.fb[k * m.bstride + b] = Fl[k];
+    else a.fb32[k * m.bstride + b] = Fl[k];
   }
 }
 

@@ -23,10 +23,16 @@ __global__ void __launch_bounds__(256) prim_kernel(int n, int st, const double* 
 static inline int grid_for(int n, int block) { return (n + block - 1) / block; }
 
 void launch_gradient_ref(const MeshView<double>& m, const StageArgs& a, Launch l) {
-  gradient_limiter_kernel<double, true><<<grid_for(4 * m.n, l.block), l.block, 0, l.stream>>>(m, a);
+  gradient_limiter_kernel<double, true><<<grid_for(5 * m.n, l.block), l.block, 0, l.stream>>>(m, a);
 }
 void launch_flux_ref(const MeshView<double>& m, const StageArgs& a, Launch l) {
   flux_update_kernel<double, true><<<grid_for(4 * m.n, l.block), l.block, 0, l.stream>>>(m, a);
+}
+void launch_ghost_ref(const MeshView<double>& m, const StageArgs& a, Launch l) {
+  if (m.nb > 0) ghost_kernel<double, true><<<grid_for(m.nb, l.block), l.block, 0, l.stream>>>(m, a);
+}
+void launch_bflux_ref(const MeshView<double>& m, const StageArgs& a, Launch l) {
+  if (m.nb > 0) boundary_flux_kernel<double, true><<<grid_for(m.nb, l.block), l.block, 0, l.stream>>>(m, a);
 }
 void launch_timestep(const MeshView<double>& m, const DtArgs& a, Launch l) {
   timestep_kernel<true><<<grid_for(m.n, l.block), l.block, 0, l.stream>>>(m, a);

@@ -12,11 +12,14 @@ namespace nf {
 struct Launch {
   int block;
   cudaStream_t stream;
+  int variant = 0;  // fast kernels: 0 one load chain at a time, 1 software-pipelined
 };
 
 // reference-order FP64 (kernels_ref.cu)
 void launch_gradient_ref(const MeshView<double>& m, const StageArgs& a, Launch l);
 void launch_flux_ref(const MeshView<double>& m, const StageArgs& a, Launch l);
+void launch_ghost_ref(const MeshView<double>& m, const StageArgs& a, Launch l);
+void launch_bflux_ref(const MeshView<double>& m, const StageArgs& a, Launch l);
 void launch_timestep(const MeshView<double>& m, const DtArgs& a, Launch l);
 void launch_prim_ref(int n, int stride, const double* U, double* V, float* V32, Launch l);
 
@@ -25,6 +28,10 @@ void launch_gradient_fast(const MeshView<double>& m, const StageArgs& a, Launch 
 void launch_flux_fast(const MeshView<double>& m, const StageArgs& a, Launch l);
 void launch_gradient_mixed(const MeshView<float>& m, const StageArgs& a, Launch l);
 void launch_flux_mixed(const MeshView<float>& m, const StageArgs& a, Launch l);
+void launch_ghost_fast(const MeshView<double>& m, const StageArgs& a, Launch l);
+void launch_bflux_fast(const MeshView<double>& m, const StageArgs& a, Launch l);
+void launch_ghost_mixed(const MeshView<float>& m, const StageArgs& a, Launch l);
+void launch_bflux_mixed(const MeshView<float>& m, const StageArgs& a, Launch l);
 void launch_prim_fast(int n, int stride, const double* U, double* V, float* V32, Launch l);
 
 }  // namespace nf

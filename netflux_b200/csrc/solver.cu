@@ -160,13 +160,14 @@ struct nf_solver {
   std::string err;
 
   // mesh
-  DevBuf<int> slot, nbslot;
-  DevBuf<double> S, nhat, area, ri, rj, vol, dS;
-  DevBuf<float> S32, nhat32, area32, ri32, rj32;
+  DevBuf<int> slot, nbslot, nbv, b_cell, b_slot, b_face, b_patch;
+  DevBuf<double> S, nhat, area, rs, sg, hvinv, vol, dS;
+  DevBuf<float> S32, nhat32, area32, rs32, sg32, hvinv32;
+  int nb = 0, bstride = 0;
   DevBuf<nf::PatchBC> patches;
   // state
-  DevBuf<double> U, W, V0, V1, fs, grad, phi, R, dt_local, res_cell, scal, part, res_out;
-  DevBuf<float> V32a, V32b, fs32, grad32, phi32;
+  DevBuf<double> U, W, V0, V1, fs, grad, phi, R, dt_local, res_cell, scal, part, res_out, vg, fb;
+  DevBuf<float> V32a, V32b, fs32, grad32, phi32, vg32, fb32;
   DevBuf<unsigned> status;
   DevBuf<long long> chunk_begin, chunk_end, case_cells;
   DevBuf<int> case_chunk0;
@@ -175,6 +176,13 @@ struct nf_solver {
   int vcur = 0;              // V buffer holding the primitives of the current state
   bool stepped = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two steps from vcur = 0 / 1
+  // launch configuration of the gradient and flux kernels (fast forms)
+  struct KCfg {
+    int block = 128;
+    int variant = 0;
+  };
+  KCfg kgrad, kflux;
+  bool tuned = false;
   DevBuf<double> stage;           // AoS staging for state transfers [N][5]
   DevBuf<long long> d_dev_of_ref;  // [N]
 
@@ -207,12 +215,12 @@ struct nf_solver {
   nf::Launch launch() const { return nf::Launch{block, stream}; }
 
   nf::MeshView<double> view64() const {
-    return nf::MeshView<double>{n, stride, n_faces, slot.p, nbslot.p, S.p, nhat.p, area.p, ri.p, rj.p,
-                                vol.p, dS.p, patches.p};
+    return nf::MeshView<double>{n, stride, n_faces, slot.p, nbslot.p, S.p, nhat.p, area.p, rs.p, sg.p, nbv.p,
+                                hvinv.p, vol.p, dS.p, patches.p, nb, bstride, b_cell.p, b_slot.p, b_face.p, b_patch.p};
   }
   nf::MeshView<float> view32() const {
-    return nf::MeshView<float>{n, stride, n_faces, slot.p, nbslot.p, S32.p, nhat32.p, area32.p, ri32.p, rj32.p,
-                               vol.p, dS.p, patches.p};
+    return nf::MeshView<float>{n, stride, n_faces, slot.p, nbslot.p, S32.p, nhat32.p, area32.p, rs32.p, sg32.p, nbv.p,
+                               hvinv32.p, vol.p, dS.p, patches.p, nb, bstride, b_cell.p, b_slot.p, b_face.p, b_patch.p};
   }
 
   void enqueue_dt() {
@@ -231,6 +239,120 @@ struct nf_solver {
     prof_end();
   }
 
+  void launch_gradient(const nf::StageArgs& a, const KCfg& k) {
+    const nf::Launch l{k.block, stream, k.variant};
+    if (p.precision == NF_PREC_MIXED) nf::launch_gradient_mixed(view32(), a, l);
+    else if (p.precision == NF_PREC_FP64) nf::launch_gradient_fast(view64(), a, l);
+    else nf::launch_gradient_ref(view64(), a, launch());
+  }
+  void launch_flux(const nf::StageArgs& a, const KCfg& k) {
+    const nf::Launch l{k.block, stream, k.variant};
+    if (p.precision == NF_PREC_MIXED) nf::launch_flux_mixed(view32(), a, l);
+    else if (p.precision == NF_PREC_FP64) nf::launch_flux_fast(view64(), a, l);
+    else nf::launch_flux_ref(view64(), a, launch());
+  }
+
+  // Arguments of the first stage of a step from the current state, writing
+  // only scratch (face states, W, the other primitive buffer).
+  nf::StageArgs first_stage_args() {
+    nf::StageArgs a{};
+    a.second_order = p.spatial_order == NF_SECOND_ORDER;
+    a.barth = p.limiter == NF_LIMITER_BARTH;
+    a.scheme = p.time_scheme == NF_TVD_RK3 ? 1 : 0;
+    a.stage = 0;
+    a.local_dt = p.local_time_stepping;
+    a.Vin = Vbuf(vcur);
+    a.Vout = Vbuf(1 - vcur);
+    a.fs = fs.p;
+    a.vg = vg.p;
+    a.fb = fb.p;
+    a.vg32 = vg32.p;
+    a.fb32 = fb32.p;
+    a.dt_local = dt_local.p;
+    a.scal = scal.p;
+    a.status = status.p;
+    a.Uin = U.p;
+    a.Uout = W.p;
+    if (p.precision == NF_PREC_MIXED) {
+      a.Vin32 = V32buf(vcur);
+      a.Vout32 = V32buf(1 - vcur);
+      a.fs32 = fs32.p;
+    }
+    return a;
+  }
+
+  // Pick block size and variant of the gradient and flux kernels by timing
+  // each candidate on the current state (CUDA events on this stream).
+  void tune() {
+    tuned = true;
+    if (p.precision == NF_PREC_FP64_REF) return;  // reference form: fixed shape
+    const int other = 1 - vcur;
+    std::vector<double> keep(size_t(5) * stride);
+    ck(cudaMemcpyAsync(keep.data(), Vbuf(other), keep.size() * sizeof(double), cudaMemcpyDeviceToHost, stream),
+       "tune save");
+    std::vector<float> keep32;
+    if (p.precision == NF_PREC_MIXED) {
+      keep32.resize(size_t(5) * stride);
+      ck(cudaMemcpyAsync(keep32.data(), V32buf(other), keep32.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                         stream),
+         "tune save");
+    }
+    ck(cudaStreamSynchronize(stream), "tune sync");
+    nf::StageArgs a = first_stage_args();
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "cudaEventCreate");
+    ck(cudaEventCreate(&e1), "cudaEventCreate");
+    auto time_it = [&](auto&& fn) {
+      fn();  // warm
+      ck(cudaEventRecord(e0, stream), "cudaEventRecord");
+      for (int r = 0; r < 3; r++) fn();
+      ck(cudaEventRecord(e1, stream), "cudaEventRecord");
+      ck(cudaEventSynchronize(e1), "cudaEventSynchronize");
+      float ms = 0.f;
+      ck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+      return ms;
+    };
+    const KCfg cands[] = {{128, 0}, {128, 1}, {64, 0}, {64, 1}};
+    if (a.second_order) {
+      if (p.precision == NF_PREC_MIXED) nf::launch_ghost_mixed(view32(), a, launch());
+      else nf::launch_ghost_fast(view64(), a, launch());
+      float best = 1e30f;
+      for (const KCfg& k : cands) {
+        const float t = time_it([&] { launch_gradient(a, k); });
+        if (t < best) {
+          best = t;
+          kgrad = k;
+        }
+      }
+      launch_gradient(a, kgrad);
+    }
+    if (p.precision == NF_PREC_MIXED) nf::launch_bflux_mixed(view32(), a, launch());
+    else nf::launch_bflux_fast(view64(), a, launch());
+    float best = 1e30f;
+    for (const KCfg& k : cands) {
+      const float t = time_it([&] { launch_flux(a, k); });
+      if (t < best) {
+        best = t;
+        kflux = k;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ck(cudaMemcpyAsync(Vbuf(other), keep.data(), keep.size() * sizeof(double), cudaMemcpyHostToDevice, stream),
+       "tune restore");
+    if (!keep32.empty())
+      ck(cudaMemcpyAsync(V32buf(other), keep32.data(), keep32.size() * sizeof(float), cudaMemcpyHostToDevice,
+                         stream),
+         "tune restore");
+    ck(cudaMemsetAsync(status.p, 0, sizeof(unsigned), stream), "status reset");
+    ck(cudaStreamSynchronize(stream), "tune sync");
+    for (auto& g : graph)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  }
+
   void enqueue_step() {
     const int n_stages = p.time_scheme == NF_TVD_RK3 ? 3 : 1;
     for (int s = 0; s < n_stages; s++) {
@@ -243,6 +365,10 @@ struct nf_solver {
       a.Vin = Vbuf(vcur);
       a.Vout = Vbuf(1 - vcur);
       a.fs = fs.p;
+      a.vg = vg.p;
+      a.fb = fb.p;
+      a.vg32 = vg32.p;
+      a.fb32 = fb32.p;
       a.grad = p.keep_stage_fields ? grad.p : nullptr;
       a.phi = p.keep_stage_fields ? phi.p : nullptr;
       a.R = p.keep_stage_fields ? R.p : nullptr;
@@ -273,16 +399,22 @@ struct nf_solver {
         a.phi32 = p.keep_stage_fields ? phi32.p : nullptr;
       }
       if (a.second_order) {
+        prof_begin(NF_KERNEL_OTHER);
+        if (p.precision == NF_PREC_MIXED) nf::launch_ghost_mixed(view32(), a, launch());
+        else if (p.precision == NF_PREC_FP64) nf::launch_ghost_fast(view64(), a, launch());
+        else nf::launch_ghost_ref(view64(), a, launch());
+        prof_end();
         prof_begin(NF_KERNEL_GRADIENT);
-        if (p.precision == NF_PREC_MIXED) nf::launch_gradient_mixed(view32(), a, launch());
-        else if (p.precision == NF_PREC_FP64) nf::launch_gradient_fast(view64(), a, launch());
-        else nf::launch_gradient_ref(view64(), a, launch());
+        launch_gradient(a, kgrad);
         prof_end();
       }
+      prof_begin(NF_KERNEL_OTHER);
+      if (p.precision == NF_PREC_MIXED) nf::launch_bflux_mixed(view32(), a, launch());
+      else if (p.precision == NF_PREC_FP64) nf::launch_bflux_fast(view64(), a, launch());
+      else nf::launch_bflux_ref(view64(), a, launch());
+      prof_end();
       prof_begin(NF_KERNEL_FLUX);
-      if (p.precision == NF_PREC_MIXED) nf::launch_flux_mixed(view32(), a, launch());
-      else if (p.precision == NF_PREC_FP64) nf::launch_flux_fast(view64(), a, launch());
-      else nf::launch_flux_ref(view64(), a, launch());
+      launch_flux(a, kflux);
       prof_end();
       vcur = 1 - vcur;
     }
@@ -511,6 +643,10 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     s->p = p;
     s->p.patches = nullptr;  // copied below
     s->block = p.block_size > 0 ? p.block_size : 256;
+    if (p.block_size > 0) {
+      s->kgrad.block = s->kflux.block = std::min(p.block_size, 128);
+      s->tuned = true;  // a caller-fixed shape is not tuned
+    }
     if (s->block % 32 || s->block > 256) throw std::runtime_error("block_size must be a multiple of 32, <= 256");
     ck(cudaGetDevice(&s->device), "cudaGetDevice");
     ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -540,20 +676,24 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     std::vector<int64_t> fdev(static_cast<size_t>(F));
     for (int64_t k = 0; k < F; k++) fdev[size_t(dev_face_order[size_t(k)])] = k;
 
-    std::vector<double> h_S(size_t(3 * F)), h_n(size_t(3 * F)), h_a(static_cast<size_t>(F)), h_ri(size_t(3 * F)),
-        h_rj(size_t(3 * F));
+    std::vector<double> h_S(size_t(3 * F)), h_n(size_t(3 * F)), h_a(static_cast<size_t>(F));
     for (int64_t f = 0; f < F; f++) {
       const int64_t d = fdev[size_t(f)];
       h_a[size_t(d)] = m.area[size_t(f)];
       for (int c = 0; c < 3; c++) {
         h_S[size_t(c * F + d)] = m.S[size_t(3 * f + c)];
         h_n[size_t(c * F + d)] = m.nhat[size_t(3 * f + c)];
-        h_ri[size_t(c * F + d)] = m.ri[size_t(3 * f + c)];
-        h_rj[size_t(c * F + d)] = m.rj[size_t(3 * f + c)];
       }
     }
     // slots in reference face order; nbslot names the other side of each face
     std::vector<int> h_slot(size_t(4) * stride, -1), h_nb(size_t(4) * stride, 0);
+    std::vector<double> h_rs(size_t(12) * stride, 0.0);  // [d][q][cell]
+    std::vector<double> h_sg(size_t(12) * stride, 0.0);  // [d][q][cell], outward normal of each slot
+    struct BFace {
+      int64_t cell;
+      int q, face, patch;
+    };
+    std::vector<BFace> bfaces;
     std::vector<int> fill(static_cast<size_t>(stride), 0);
     auto add_slot = [&](int64_t cell_dev, int value) {
       int& k = fill[size_t(cell_dev)];
@@ -565,20 +705,52 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
       const int fd = int(fdev[size_t(f)]);
       const int64_t di = m.dev_of_ref[m.face_i[size_t(f)]];
       const int qi = add_slot(di, fd << 1);
+      for (int c = 0; c < 3; c++) {
+        h_rs[(size_t(c) * 4 + qi) * stride + size_t(di)] = m.ri[size_t(3 * f + c)];
+        h_sg[(size_t(c) * 4 + qi) * stride + size_t(di)] = m.S[size_t(3 * f + c)];
+      }
       const uint32_t j = m.face_j[size_t(f)];
       if (j < uint32_t(N)) {
         const int64_t dj = m.dev_of_ref[j];
         const int qj = add_slot(dj, (fd << 1) | 1);
+        for (int c = 0; c < 3; c++) {
+          h_rs[(size_t(c) * 4 + qj) * stride + size_t(dj)] = m.rj[size_t(3 * f + c)];
+          h_sg[(size_t(c) * 4 + qj) * stride + size_t(dj)] = -m.S[size_t(3 * f + c)];
+        }
         h_nb[size_t(qi) * stride + size_t(di)] = int(dj << 2) | qj;
         h_nb[size_t(qj) * stride + size_t(dj)] = int(di << 2) | qi;
       } else {
-        h_nb[size_t(qi) * stride + size_t(di)] = -(1 + m.face_patch[size_t(f)]);
+        bfaces.push_back({di, qi, fd, int(m.face_patch[size_t(f)])});
       }
     }
-    std::vector<double> h_vol(size_t(stride), 1.0), h_dS(size_t(3) * stride, 0.0);
+    // boundary faces in owner-cell order; the owner's slot names its index
+    std::stable_sort(bfaces.begin(), bfaces.end(), [](const BFace& x, const BFace& y) { return x.cell < y.cell; });
+    const int nbf = int(bfaces.size());
+    std::vector<int> hb_cell(static_cast<size_t>(nbf)), hb_slot(static_cast<size_t>(nbf)), hb_face(static_cast<size_t>(nbf)), hb_patch(static_cast<size_t>(nbf));
+    for (int b = 0; b < nbf; b++) {
+      hb_cell[size_t(b)] = int(bfaces[size_t(b)].cell);
+      hb_slot[size_t(b)] = bfaces[size_t(b)].q;
+      hb_face[size_t(b)] = bfaces[size_t(b)].face;
+      hb_patch[size_t(b)] = bfaces[size_t(b)].patch;
+      h_nb[size_t(bfaces[size_t(b)].q) * stride + size_t(bfaces[size_t(b)].cell)] = -(1 + b);
+    }
+    // neighbour of each slot for the fast gradient: cell, -(1 + boundary face),
+    // or the cell itself where the slot holds no face
+    std::vector<int> h_nbv(size_t(4) * stride, 0);
+    for (int q = 0; q < 4; q++)
+      for (int64_t c = 0; c < stride; c++) {
+        const size_t i = size_t(q) * stride + size_t(c);
+        if (c >= N || h_slot[i] < 0) h_nbv[i] = int(std::min<int64_t>(c, N - 1));
+        else h_nbv[i] = h_nb[i] >= 0 ? (h_nb[i] >> 2) : h_nb[i];
+      }
+    s->nb = nbf;
+    s->bstride = std::max(64, (nbf + 63) / 64 * 64);
+    std::vector<double> h_vol(size_t(stride), 1.0), h_dS(size_t(3) * stride, 0.0),
+        h_hv(size_t(stride), 0.5);
     for (int64_t c = 0; c < N; c++) {
       const int64_t d = m.dev_of_ref[size_t(c)];
       h_vol[size_t(d)] = m.vol[size_t(c)];
+      h_hv[size_t(d)] = 0.5 / m.vol[size_t(c)];
       for (int k = 0; k < 3; k++) h_dS[size_t(k) * stride + size_t(d)] = m.dS[size_t(3 * c + k)];
     }
     // boundary conditions per patch
@@ -597,12 +769,18 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
 
     s->slot.upload(h_slot, st);
     s->nbslot.upload(h_nb, st);
+    s->b_cell.upload(hb_cell, st);
+    s->b_slot.upload(hb_slot, st);
+    s->b_face.upload(hb_face, st);
+    s->b_patch.upload(hb_patch, st);
+    s->rs.upload(h_rs, st);
+    s->sg.upload(h_sg, st);
+    s->nbv.upload(h_nbv, st);
     s->S.upload(h_S, st);
     s->nhat.upload(h_n, st);
     s->area.upload(h_a, st);
-    s->ri.upload(h_ri, st);
-    s->rj.upload(h_rj, st);
     s->vol.upload(h_vol, st);
+    s->hvinv.upload(h_hv, st);
     s->dS.upload(h_dS, st);
     s->patches.upload(h_pb, st);
     if (p.precision == NF_PREC_MIXED) {
@@ -614,8 +792,13 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
       s->S32.upload(tof(h_S), st);
       s->nhat32.upload(tof(h_n), st);
       s->area32.upload(tof(h_a), st);
-      s->ri32.upload(tof(h_ri), st);
-      s->rj32.upload(tof(h_rj), st);
+      s->rs32.upload(tof(h_rs), st);
+      s->sg32.upload(tof(h_sg), st);
+      s->hvinv32.upload(tof(h_hv), st);
+      s->vg32.alloc(size_t(5) * s->bstride);
+      s->fb32.alloc(size_t(5) * s->bstride);
+      s->vg32.zero(st);
+      s->fb32.zero(st);
       s->V32a.alloc(size_t(5) * stride);
       s->V32b.alloc(size_t(5) * stride);
       s->fs32.alloc(size_t(20) * stride);
@@ -636,6 +819,10 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     if (p.precision != NF_PREC_MIXED) {
       s->fs.alloc(size_t(20) * stride);
       s->fs.zero(st);
+      s->vg.alloc(size_t(5) * s->bstride);
+      s->fb.alloc(size_t(5) * s->bstride);
+      s->vg.zero(st);
+      s->fb.zero(st);
     }
     if (p.keep_stage_fields) {
       s->R.alloc(size_t(5) * stride);
@@ -952,6 +1139,19 @@ int nf_time_steps(nf_solver* s, int64_t n_steps, int per_kernel, double* ms_tota
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    return s->check_status();
+  });
+}
+
+int nf_tune(nf_solver* s, int* config) {
+  return guarded(s, [&]() -> int {
+    s->tune();
+    if (config) {
+      config[0] = s->kgrad.block;
+      config[1] = s->kgrad.variant;
+      config[2] = s->kflux.block;
+      config[3] = s->kflux.variant;
+    }
     return s->check_status();
   });
 }

@@ -302,6 +302,12 @@ class EulerSolver:
         _check(L.load().nf_advance(self._h, int(n_steps), C.byref(t)), self._h)
         return t.value
 
+    def tune(self):
+        """Time the gradient/flux launch shapes on the current state and keep the fastest."""
+        cfg = (C.c_int * 4)()
+        _check(L.load().nf_tune(self._h, cfg), self._h)
+        return {"gradient": {"block": cfg[0], "variant": cfg[1]}, "flux": {"block": cfg[2], "variant": cfg[3]}}
+
     def synchronize(self) -> None:
         _check(L.load().nf_synchronize(self._h), self._h)
 

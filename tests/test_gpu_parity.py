@@ -112,6 +112,23 @@ def test_advance_graph_equals_step_loop():
     assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tuning_changes_nothing(precision):
+    """Tuned launch shapes compute the same bits and leave the state untouched."""
+    g = golden("bump12")
+    cfg = config_for(precision=precision, freestream=tuple(g["freestream"]))
+    a = S.EulerSolver(cfg, mesh(g), U0=g["U0"])
+    a.advance(3)
+    b = S.EulerSolver(cfg, mesh(g), U0=g["U0"])
+    b.advance(1)
+    before = b.get_solver_data().get_solution()
+    shapes = b.tune()
+    assert np.array_equal(b.get_solver_data().get_solution(), before)
+    assert shapes["flux"]["block"] in (64, 128)
+    b.advance(2)
+    assert np.array_equal(a.get_solver_data().get_solution(), b.get_solver_data().get_solution())
+
+
 def test_deterministic_repeat():
     g = golden("sod40")
     _, a, _ = run(g, "fp64", 20, use_advance=True)
