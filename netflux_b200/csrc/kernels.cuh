@@ -47,9 +47,12 @@ struct MeshView {
   const T* __restrict__ nhat;      // [3][F]
   const T* __restrict__ area;      // [F]
   const T* __restrict__ rs;        // [3][4][stride] centroid-to-face vector of each slot
-  const T* __restrict__ sg;        // [3][4][stride] face normal seen from the cell (outward), 0 for no face
-  const int* __restrict__ nbv;     // [4][stride] neighbour cell, -(1 + boundary face), or the cell itself for no face
-  const T* __restrict__ hvinv;     // [stride] 0.5 / vol
+  // node-based geometry of the fast forms (face m = the face opposite vertex m)
+  const T* __restrict__ nodes;     // [n_nodes][4] x, y, z, 0
+  const int* __restrict__ cnode;   // [4][stride] vertices of each cell, ascending node id
+  const int* __restrict__ gcode;   // [stride] per face m, bits 3m..3m+2: present, outward flip, neighbour side
+  const int* __restrict__ nbvf;    // [4][stride] neighbour cell of face m, -(1 + boundary face), or the cell itself
+  const int* __restrict__ nbsf;    // [4][stride] neighbour << 2 | its face index, or -(1 + boundary face)
   const double* __restrict__ vol;
   const double* __restrict__ dS;
   const PatchBC* __restrict__ patches;
@@ -60,6 +63,7 @@ struct MeshView {
   const int* __restrict__ b_slot;  // owner's slot of the face
   const int* __restrict__ b_face;  // face id (geometry)
   const int* __restrict__ b_patch; // patch
+  const int* __restrict__ b_fs;    // face-state slot of the owner (slot order of the kernels in use)
 };
 
 struct StageArgs {
@@ -389,20 +393,60 @@ __global__ void __launch_bounds__(256) flux_update_kernel(MeshView<T> m, StageAr
 }
 
 // ---------------------------------------------------------------------------
-// Fast forms (FP64 with contraction, and mixed FP32): one thread per cell.
-//
-// gradient_fast_kernel: the same Green-Gauss gradient, min/max, Barth limiter
-// and reconstruction, rearranged for fewer instructions (results agree with
-// the reference form to round-off):
-//   grad V = 0.5/vol (sum_q V_q S_q + V_c sum_q S_q) with S_q the outward
-//   normal of slot q; a missing slot has S_q = 0, r_q = 0 and points at the
-//   cell itself, so it changes nothing and needs no branch;
-//   phi = min(1, min_q A_q / D_q) with A_q = (V_max - V_c) or (V_c - V_min)
-//   and D_q = |grad V . r_q| + eps: the minimising face is found by
+// Fast forms (FP64 with contraction, and mixed FP32): one thread per cell, the
+// cell's faces indexed by the vertex they face, geometry rebuilt from the
+// vertices (the node array stays in L2):
+//   * the vertices of a cell are stored sorted by node id, so face m's three
+//     vertices, taken in that order, are the same ordered triple in both cells
+//     of the face and give bit-identical normals S = 0.5 (B - A) x (C - A);
+//     a per-face bit turns S outward;
+//   * the vector from the centroid to the centroid of face m is
+//     (centroid - P_m) / 3.
+// gradient_node_kernel computes the same Green-Gauss gradient, min/max, Barth
+// limiter and reconstruction as the reference form, rearranged for fewer
+// instructions (agreement to round-off):
+//   grad V = 0.5/vol (sum_m V_m S_m + V_c sum_m S_m);
+//   phi = min(1, min_m A_m / D_m) with A_m = (V_max - V_c) or (V_c - V_min)
+//   and D_m = |grad V . r_m| + eps, the minimising face found by
 //   cross-multiplication, then one division per variable.
+// A missing face (a boundary face no marker lists) has S = r = 0 and points
+// at the cell itself, so it changes nothing.
 // ---------------------------------------------------------------------------
-template <typename T, bool kPipe>
-__global__ void __launch_bounds__(128) gradient_fast_kernel(MeshView<T> m, StageArgs a) {
+template <typename T>
+__device__ __forceinline__ void load_vertices(const MeshView<T>& m, int c, T P[4][3]) {
+#pragma unroll
+  for (int v = 0; v < 4; v++) {
+    const int id = m.cnode[v * m.stride + c];
+    const T* p = m.nodes + 4 * size_t(id);
+    P[v][0] = p[0];
+    P[v][1] = p[1];
+    P[v][2] = p[2];
+  }
+}
+
+// normal of face fm (opposite vertex fm) from its vertices in ascending order
+template <typename T, int fm>
+__device__ __forceinline__ void face_normal(const T P[4][3], T S[3]) {
+  constexpr int a = fm == 0 ? 1 : 0;
+  constexpr int b = fm <= 1 ? 2 : 1;
+  constexpr int cc = fm == 3 ? 2 : 3;
+  const T e1[3] = {P[b][0] - P[a][0], P[b][1] - P[a][1], P[b][2] - P[a][2]};
+  const T e2[3] = {P[cc][0] - P[a][0], P[cc][1] - P[a][1], P[cc][2] - P[a][2]};
+  S[0] = T(0.5) * (e1[1] * e2[2] - e1[2] * e2[1]);
+  S[1] = T(0.5) * (e1[2] * e2[0] - e1[0] * e2[2]);
+  S[2] = T(0.5) * (e1[0] * e2[1] - e1[1] * e2[0]);
+}
+
+template <typename T>
+__device__ __forceinline__ void face_normals(const T P[4][3], T S[4][3]) {
+  face_normal<T, 0>(P, S[0]);
+  face_normal<T, 1>(P, S[1]);
+  face_normal<T, 2>(P, S[2]);
+  face_normal<T, 3>(P, S[3]);
+}
+
+template <typename T, bool kPipe, int kMinBlocks>
+__global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView<T> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.n) return;
   const int st = m.stride;
@@ -420,8 +464,7 @@ __global__ void __launch_bounds__(128) gradient_fast_kernel(MeshView<T> m, Stage
   }
   int nb[4];
 #pragma unroll
-  for (int q = 0; q < 4; q++) nb[q] = m.nbv[q * st + c];
-  // the values of variable k: own and the four neighbours (or ghosts)
+  for (int q = 0; q < 4; q++) nb[q] = m.nbvf[q * st + c];
   auto fetch = [&](int k, T& vc, T vo[4]) {
     const T* Vk = Vin + k * st;
     vc = Vk[c];
@@ -430,15 +473,29 @@ __global__ void __launch_bounds__(128) gradient_fast_kernel(MeshView<T> m, Stage
   };
   T vcN, voN[4];
   if (kPipe) fetch(0, vcN, voN);
-  T sgv[4][3];
+  const int code = m.gcode[c];
+  T S[4][3], d[4][3];  // outward normals; (centroid - P_m) / 3
+  {
+    T P[4][3];
+    load_vertices(m, c, P);
+    face_normals(P, S);
+    const T cen[3] = {T(0.25) * ((P[0][0] + P[1][0]) + (P[2][0] + P[3][0])),
+                      T(0.25) * ((P[0][1] + P[1][1]) + (P[2][1] + P[3][1])),
+                      T(0.25) * ((P[0][2] + P[1][2]) + (P[2][2] + P[3][2]))};
 #pragma unroll
-  for (int q = 0; q < 4; q++)
+    for (int q = 0; q < 4; q++) {
+      const int bits = code >> (3 * q);
+      const T sgn = (bits & 1) == 0 ? T(0) : ((bits & 2) ? T(-1) : T(1));  // 0: no face
 #pragma unroll
-    for (int d = 0; d < 3; d++) sgv[q][d] = m.sg[(d * 4 + q) * st + c];
-  const T ssum[3] = {(sgv[0][0] + sgv[1][0]) + (sgv[2][0] + sgv[3][0]),
-                     (sgv[0][1] + sgv[1][1]) + (sgv[2][1] + sgv[3][1]),
-                     (sgv[0][2] + sgv[1][2]) + (sgv[2][2] + sgv[3][2])};
-  const T hv = m.hvinv[c];
+      for (int e = 0; e < 3; e++) {
+        S[q][e] *= sgn;
+        d[q][e] = (bits & 1) ? (cen[e] - P[q][e]) * T(1.0 / 3.0) : T(0);
+      }
+    }
+  }
+  const T ssum[3] = {(S[0][0] + S[1][0]) + (S[2][0] + S[3][0]), (S[0][1] + S[1][1]) + (S[2][1] + S[3][1]),
+                     (S[0][2] + S[1][2]) + (S[2][2] + S[3][2])};
+  const T hv = T(0.5 / m.vol[c]);
 #pragma unroll 1
   for (int k = 0; k < 5; k++) {
     T vc, vo[4];
@@ -452,20 +509,17 @@ __global__ void __launch_bounds__(128) gradient_fast_kernel(MeshView<T> m, Stage
     }
     T acc[3];
 #pragma unroll
-    for (int d = 0; d < 3; d++) {
-      acc[d] = vc * ssum[d];
+    for (int e = 0; e < 3; e++) {
+      acc[e] = vc * ssum[e];
 #pragma unroll
-      for (int q = 0; q < 4; q++) acc[d] = fma(vo[q], sgv[q][d], acc[d]);
+      for (int q = 0; q < 4; q++) acc[e] = fma(vo[q], S[q][e], acc[e]);
     }
     const T g[3] = {hv * acc[0], hv * acc[1], hv * acc[2]};
     const T vmax = fmax(fmax(fmax(vc, vo[0]), fmax(vo[1], vo[2])), vo[3]);
     const T vmin = fmin(fmin(fmin(vc, vo[0]), fmin(vo[1], vo[2])), vo[3]);
     T gr[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const T* r = m.rs + q * st + c;
-      gr[q] = fma(g[2], r[8 * st], fma(g[1], r[4 * st], g[0] * r[0]));
-    }
+    for (int q = 0; q < 4; q++) gr[q] = fma(g[2], d[q][2], fma(g[1], d[q][1], g[0] * d[q][0]));
     T phi = T(1);
     if (a.barth) {
       T An = T(1), Dn = T(1);  // best ratio so far, starting at 1
@@ -485,38 +539,36 @@ __global__ void __launch_bounds__(128) gradient_fast_kernel(MeshView<T> m, Stage
     if constexpr (sizeof(T) == 8) {
       if (a.grad) {
 #pragma unroll
-        for (int d = 0; d < 3; d++) a.grad[(k * 3 + d) * st + c] = g[d];
+        for (int e = 0; e < 3; e++) a.grad[(k * 3 + e) * st + c] = g[e];
         a.phi[k * st + c] = phi;
       }
     } else {
       if (a.grad32) {
 #pragma unroll
-        for (int d = 0; d < 3; d++) a.grad32[(k * 3 + d) * st + c] = g[d];
+        for (int e = 0; e < 3; e++) a.grad32[(k * 3 + e) * st + c] = g[e];
         a.phi32[k * st + c] = phi;
       }
     }
   }
 }
 
-// flux_fast_kernel: the flux balance and stage update of one cell per thread.
-// Interior faces use the two face states; boundary faces add the flux that
-// boundary_flux_kernel computed. The next face's loads are issued before the
-// current face's flux is evaluated.
+// flux_node_kernel: flux balance and stage update of one cell per thread.
+// Each interior face's flux is evaluated with the reference's owner on the
+// left and the owner-to-neighbour unit normal, which both cells rebuild to the
+// same bits, so both add exactly opposite contributions; boundary faces add
+// the flux boundary_flux_kernel computed.
 template <typename T>
-struct FaceInput {
+struct FaceIn {
   T s[5];      // this cell's face state, or the boundary flux
   T x[5];      // the other side's face state
-  T n[3];
-  T area;
   int kind;    // 0 no face, 1 interior (owner), 2 interior (neighbour side), 3 boundary
 };
 
-template <typename T, bool kPipe>
-__global__ void __launch_bounds__(128) flux_fast_kernel(MeshView<T> m, StageArgs a) {
+template <typename T, bool kPipe, int kMinBlocks>
+__global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.n) return;
   const int st = m.stride;
-  const int F = m.n_faces;
   const bool second = a.second_order != 0;
   const T* fsb = nullptr;
   const T* Vin = nullptr;
@@ -530,41 +582,41 @@ __global__ void __launch_bounds__(128) flux_fast_kernel(MeshView<T> m, StageArgs
     Vin = reinterpret_cast<const T*>(a.Vin32);
     fb = reinterpret_cast<const T*>(a.fb32);
   }
-  int sl[4], ns[4];
+  const int code = m.gcode[c];
+  int ns[4];
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    sl[q] = m.slot[q * st + c];
-    ns[q] = m.nbslot[q * st + c];
-  }
-  auto fetch = [&](int q, FaceInput<T>& in) {
-    const int s_ = sl[q], n_ = ns[q];
-    if (s_ < 0) {
+  for (int q = 0; q < 4; q++) ns[q] = m.nbsf[q * st + c];
+  auto fetch = [&](int q, FaceIn<T>& in) {
+    const int bits = code >> (3 * q);
+    if ((bits & 1) == 0) {
       in.kind = 0;
-    } else if (n_ < 0) {
+    } else if (ns[q] < 0) {
       in.kind = 3;
-      const int b = -n_ - 1;
+      const int b = -ns[q] - 1;
 #pragma unroll
       for (int k = 0; k < 5; k++) in.s[k] = fb[k * m.bstride + b];
     } else {
-      const int f = s_ >> 1, o = n_ >> 2, q2 = n_ & 3;
-      in.kind = (s_ & 1) ? 2 : 1;
+      const int o = ns[q] >> 2, q2 = ns[q] & 3;
+      in.kind = (bits & 4) ? 2 : 1;
 #pragma unroll
       for (int k = 0; k < 5; k++) {
         in.s[k] = second ? fsb[(q * 5 + k) * st + c] : Vin[k * st + c];
         in.x[k] = second ? fsb[(q2 * 5 + k) * st + o] : Vin[k * st + o];
       }
-      in.n[0] = m.nhat[f];
-      in.n[1] = m.nhat[F + f];
-      in.n[2] = m.nhat[2 * F + f];
-      in.area = m.area[f];
     }
   };
-  double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  FaceInput<T> nxt;
+  FaceIn<T> nxt;
   if (kPipe) fetch(0, nxt);
-#pragma unroll 1
+  T S[4][3];
+  {
+    T P[4][3];
+    load_vertices(m, c, P);
+    face_normals(P, S);
+  }
+  double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
   for (int q = 0; q < 4; q++) {
-    FaceInput<T> cur;
+    FaceIn<T> cur;
     if (kPipe) {
       cur = nxt;
       if (q < 3) fetch(q + 1, nxt);  // next face's loads overlap this face's flux
@@ -575,10 +627,18 @@ __global__ void __launch_bounds__(128) flux_fast_kernel(MeshView<T> m, StageArgs
 #pragma unroll
       for (int k = 0; k < 5; k++) R[k] -= double(cur.s[k]);
     } else if (cur.kind != 0) {
+      const int bits = code >> (3 * q);
       const bool own = cur.kind == 1;
+      // owner-to-neighbour normal: this cell's outward normal on the owner side
+      const bool flip = own ? (bits & 2) != 0 : (bits & 2) == 0;
+      const T a2 = (S[q][0] * S[q][0] + S[q][1] * S[q][1]) + S[q][2] * S[q][2];
+      const T area = sqrt(a2);
+      const T inv = T(1) / area;
+      const T sg = flip ? -inv : inv;
+      const T nh[3] = {S[q][0] * sg, S[q][1] * sg, S[q][2] * sg};
       T Fl[5];
-      if (own) rusanov_fast<T>(cur.s, cur.x, cur.n, cur.area, Fl);
-      else rusanov_fast<T>(cur.x, cur.s, cur.n, cur.area, Fl);
+      if (own) rusanov_fast<T>(cur.s, cur.x, nh, area, Fl);
+      else rusanov_fast<T>(cur.x, cur.s, nh, area, Fl);
 #pragma unroll
       for (int k = 0; k < 5; k++) R[k] = own ? R[k] - double(Fl[k]) : R[k] + double(Fl[k]);
     }
@@ -646,7 +706,7 @@ template <typename T, bool kRef>
 __global__ void __launch_bounds__(256) boundary_flux_kernel(MeshView<T> m, StageArgs a) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= m.nb) return;
-  const int c = m.b_cell[b], q = m.b_slot[b], f = m.b_face[b];
+  const int c = m.b_cell[b], q = m.b_fs[b], f = m.b_face[b];
   const int F = m.n_faces, st = m.stride;
   T VL[5], VR[5];
 #pragma unroll

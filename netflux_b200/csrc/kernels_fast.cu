@@ -25,25 +25,34 @@ static inline int grid_for(int n, int block) { return (n + block - 1) / block; }
 // one thread per cell, at most 128 threads per block (the kernels' launch bounds)
 static inline int fast_block(int b) { return b > 128 ? 128 : b; }
 
+// Variants (the tuner times them): 0 plain, 1 software-pipelined, 2 plain
+// with registers capped for at least kCap resident 128-thread blocks per SM
+// (6 for FP64, 8 for FP32), 3 pipelined with the same cap.
+template <typename T>
+constexpr int kCap = sizeof(T) == 8 ? 6 : 8;
+#define NF_NODE_DISPATCH(KERNEL, T, m, a, l)                                                       \
+  do {                                                                                              \
+    const int b = fast_block(l.block);                                                             \
+    const int g = grid_for(m.n, b);                                                                \
+    switch (l.variant) {                                                                            \
+      case 1: KERNEL<T, true, 1><<<g, b, 0, l.stream>>>(m, a); break;                             \
+      case 2: KERNEL<T, false, kCap<T>><<<g, b, 0, l.stream>>>(m, a); break;                          \
+      case 3: KERNEL<T, true, kCap<T>><<<g, b, 0, l.stream>>>(m, a); break;                           \
+      default: KERNEL<T, false, 1><<<g, b, 0, l.stream>>>(m, a); break;                           \
+    }                                                                                               \
+  } while (0)
+
 void launch_gradient_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
-  const int b = fast_block(l.block);
-  if (l.variant == 1) gradient_fast_kernel<double, true><<<grid_for(m.n, b), b, 0, l.stream>>>(m, a);
-  else gradient_fast_kernel<double, false><<<grid_for(m.n, b), b, 0, l.stream>>>(m, a);
+  NF_NODE_DISPATCH(gradient_node_kernel, double, m, a, l);
 }
 void launch_flux_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
-  const int b = fast_block(l.block);
-  if (l.variant == 1) flux_fast_kernel<double, true><<<grid_for(m.n, b), b, 0, l.stream>>>(m, a);
-  else flux_fast_kernel<double, false><<<grid_for(m.n, b), b, 0, l.stream>>>(m, a);
+  NF_NODE_DISPATCH(flux_node_kernel, double, m, a, l);
 }
 void launch_gradient_mixed(const MeshView<float>& m, const StageArgs& a, Launch l) {
-  const int b = fast_block(l.block);
-  if (l.variant == 1) gradient_fast_kernel<float, true><<<grid_for(m.n, b), b, 0, l.stream>>>(m, a);
-  else gradient_fast_kernel<float, false><<<grid_for(m.n, b), b, 0, l.stream>>>(m, a);
+  NF_NODE_DISPATCH(gradient_node_kernel, float, m, a, l);
 }
 void launch_flux_mixed(const MeshView<float>& m, const StageArgs& a, Launch l) {
-  const int b = fast_block(l.block);
-  if (l.variant == 1) flux_fast_kernel<float, true><<<grid_for(m.n, b), b, 0, l.stream>>>(m, a);
-  else flux_fast_kernel<float, false><<<grid_for(m.n, b), b, 0, l.stream>>>(m, a);
+  NF_NODE_DISPATCH(flux_node_kernel, float, m, a, l);
 }
 void launch_ghost_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
   if (m.nb > 0) ghost_kernel<double, false><<<grid_for(m.nb, l.block), l.block, 0, l.stream>>>(m, a);

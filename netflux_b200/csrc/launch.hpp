@@ -12,7 +12,7 @@ namespace nf {
 struct Launch {
   int block;
   cudaStream_t stream;
-  int variant = 0;  // fast kernels: 0 one load chain at a time, 1 software-pipelined
+  int variant = 0;  // fast kernels: bit 0 software-pipelined, bit 1 registers capped for occupancy
 };
 
 // reference-order FP64 (kernels_ref.cu)

@@ -259,7 +259,9 @@ Mesh build_mesh(const std::vector<double>& nodes, const std::vector<int64_t>& te
   m.rj.resize(size_t(3 * F));
   m.nhat.resize(size_t(3 * F));
   m.area.resize(static_cast<size_t>(F));
+  m.face_nodes.resize(size_t(3 * F));
   auto face_geometry = [&](int64_t f, uint32_t i, uint32_t j, const uint32_t fn[3]) {
+    for (int q = 0; q < 3; q++) m.face_nodes[size_t(3 * f + q)] = fn[q];
     const V3 n0 = node(nodes, fn[0]), n1 = node(nodes, fn[1]), n2 = node(nodes, fn[2]);
     V3 S = scale(0.5, cross(sub(n1, n0), sub(n2, n0)));  // triangle_calc_face_normal
     const V3 fc = {((n0[0] + n1[0]) + n2[0]) / 3, ((n0[1] + n1[1]) + n2[1]) / 3, ((n0[2] + n1[2]) + n2[2]) / 3};
@@ -316,6 +318,8 @@ Mesh build_mesh(const std::vector<double>& nodes, const std::vector<int64_t>& te
     }
   }
 
+  m.nodes = nodes;
+  m.tet = std::move(tet);
   m.dev_of_ref.resize(static_cast<size_t>(N));
   m.ref_of_dev.resize(static_cast<size_t>(N));
   m.case_offsets = {0, N};
@@ -443,9 +447,12 @@ Mesh concat_meshes(const std::vector<const Mesh*>& parts) {
   m.centroid.assign(size_t(3 * (NC + NG)), 0.0);
   m.dS.reserve(size_t(3 * NC));
   m.case_offsets.assign(1, 0);
-  int64_t cell0 = 0, ghost0 = NC, face0 = 0;
+  int64_t cell0 = 0, ghost0 = NC, face0 = 0, node0 = 0;
   int case_index = 0;
   for (const Mesh* p : parts) {
+    m.nodes.insert(m.nodes.end(), p->nodes.begin(), p->nodes.end());
+    for (uint32_t v : p->tet) m.tet.push_back(uint32_t(node0 + v));
+    for (uint32_t v : p->face_nodes) m.face_nodes.push_back(uint32_t(node0 + v));
     for (int c = 0; c < p->n_cases(); c++) m.case_offsets.push_back(cell0 + p->case_offsets[size_t(c + 1)]);
     for (int64_t f = 0; f < p->n_faces; f++) {
       const uint32_t i = p->face_i[size_t(f)], j = p->face_j[size_t(f)];
@@ -482,6 +489,7 @@ Mesh concat_meshes(const std::vector<const Mesh*>& parts) {
     cell0 += p->n_cells;
     ghost0 += p->n_ghost();
     face0 += p->n_faces;
+    node0 += p->n_nodes;
     case_index += p->n_cases();
   }
   // interior-face count is per case; the batched face list interleaves them,

@@ -39,6 +39,11 @@ struct Mesh {
   // Per cell incl. ghosts: volume (0 for ghosts) and centroid.
   std::vector<double> vol, centroid;
   std::vector<double> dS;           // [n_cells][3], Blazek's projected areas
+
+  // Primal data kept for the node-based geometry of the fast kernels.
+  std::vector<double> nodes;        // [n_nodes][3]
+  std::vector<uint32_t> tet;        // [n_cells][4] node ids after the reader's 1<->2 swap
+  std::vector<uint32_t> face_nodes; // [F][3] node ids of each face element
   std::vector<Patch> patches;
 
   // Device numbering (Hilbert order of centroids, per case).

@@ -160,9 +160,10 @@ struct nf_solver {
   std::string err;
 
   // mesh
-  DevBuf<int> slot, nbslot, nbv, b_cell, b_slot, b_face, b_patch;
-  DevBuf<double> S, nhat, area, rs, sg, hvinv, vol, dS;
-  DevBuf<float> S32, nhat32, area32, rs32, sg32, hvinv32;
+  DevBuf<int> slot, nbslot, b_cell, b_slot, b_face, b_patch, b_slotf;
+  DevBuf<int> cnode, gcode, nbvf, nbsf;  // node-based layout of the fast forms
+  DevBuf<double> S, nhat, area, rs, vol, dS, nodes4;
+  DevBuf<float> S32, nhat32, area32, rs32, nodes4_32;
   int nb = 0, bstride = 0;
   DevBuf<nf::PatchBC> patches;
   // state
@@ -215,12 +216,15 @@ struct nf_solver {
   nf::Launch launch() const { return nf::Launch{block, stream}; }
 
   nf::MeshView<double> view64() const {
-    return nf::MeshView<double>{n, stride, n_faces, slot.p, nbslot.p, S.p, nhat.p, area.p, rs.p, sg.p, nbv.p,
-                                hvinv.p, vol.p, dS.p, patches.p, nb, bstride, b_cell.p, b_slot.p, b_face.p, b_patch.p};
+    const bool fast = p.precision != NF_PREC_FP64_REF;
+    return nf::MeshView<double>{n, stride, n_faces, slot.p, nbslot.p, S.p, nhat.p, area.p, rs.p,
+                                nodes4.p, cnode.p, gcode.p, nbvf.p, nbsf.p, vol.p, dS.p, patches.p, nb,
+                                bstride, b_cell.p, b_slot.p, b_face.p, b_patch.p, fast ? b_slotf.p : b_slot.p};
   }
   nf::MeshView<float> view32() const {
-    return nf::MeshView<float>{n, stride, n_faces, slot.p, nbslot.p, S32.p, nhat32.p, area32.p, rs32.p, sg32.p, nbv.p,
-                               hvinv32.p, vol.p, dS.p, patches.p, nb, bstride, b_cell.p, b_slot.p, b_face.p, b_patch.p};
+    return nf::MeshView<float>{n, stride, n_faces, slot.p, nbslot.p, S32.p, nhat32.p, area32.p, rs32.p,
+                               nodes4_32.p, cnode.p, gcode.p, nbvf.p, nbsf.p, vol.p, dS.p, patches.p, nb,
+                               bstride, b_cell.p, b_slot.p, b_face.p, b_patch.p, b_slotf.p};
   }
 
   void enqueue_dt() {
@@ -312,7 +316,7 @@ struct nf_solver {
       ck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
       return ms;
     };
-    const KCfg cands[] = {{128, 0}, {128, 1}, {64, 0}, {64, 1}};
+    const KCfg cands[] = {{128, 0}, {128, 1}, {128, 2}, {128, 3}, {64, 0}, {64, 1}, {64, 2}, {64, 3}};
     if (a.second_order) {
       if (p.precision == NF_PREC_MIXED) nf::launch_ghost_mixed(view32(), a, launch());
       else nf::launch_ghost_fast(view64(), a, launch());
@@ -688,7 +692,6 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     // slots in reference face order; nbslot names the other side of each face
     std::vector<int> h_slot(size_t(4) * stride, -1), h_nb(size_t(4) * stride, 0);
     std::vector<double> h_rs(size_t(12) * stride, 0.0);  // [d][q][cell]
-    std::vector<double> h_sg(size_t(12) * stride, 0.0);  // [d][q][cell], outward normal of each slot
     struct BFace {
       int64_t cell;
       int q, face, patch;
@@ -705,18 +708,12 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
       const int fd = int(fdev[size_t(f)]);
       const int64_t di = m.dev_of_ref[m.face_i[size_t(f)]];
       const int qi = add_slot(di, fd << 1);
-      for (int c = 0; c < 3; c++) {
-        h_rs[(size_t(c) * 4 + qi) * stride + size_t(di)] = m.ri[size_t(3 * f + c)];
-        h_sg[(size_t(c) * 4 + qi) * stride + size_t(di)] = m.S[size_t(3 * f + c)];
-      }
+      for (int c = 0; c < 3; c++) h_rs[(size_t(c) * 4 + qi) * stride + size_t(di)] = m.ri[size_t(3 * f + c)];
       const uint32_t j = m.face_j[size_t(f)];
       if (j < uint32_t(N)) {
         const int64_t dj = m.dev_of_ref[j];
         const int qj = add_slot(dj, (fd << 1) | 1);
-        for (int c = 0; c < 3; c++) {
-          h_rs[(size_t(c) * 4 + qj) * stride + size_t(dj)] = m.rj[size_t(3 * f + c)];
-          h_sg[(size_t(c) * 4 + qj) * stride + size_t(dj)] = -m.S[size_t(3 * f + c)];
-        }
+        for (int c = 0; c < 3; c++) h_rs[(size_t(c) * 4 + qj) * stride + size_t(dj)] = m.rj[size_t(3 * f + c)];
         h_nb[size_t(qi) * stride + size_t(di)] = int(dj << 2) | qj;
         h_nb[size_t(qj) * stride + size_t(dj)] = int(di << 2) | qi;
       } else {
@@ -734,23 +731,94 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
       hb_patch[size_t(b)] = bfaces[size_t(b)].patch;
       h_nb[size_t(bfaces[size_t(b)].q) * stride + size_t(bfaces[size_t(b)].cell)] = -(1 + b);
     }
-    // neighbour of each slot for the fast gradient: cell, -(1 + boundary face),
-    // or the cell itself where the slot holds no face
-    std::vector<int> h_nbv(size_t(4) * stride, 0);
-    for (int q = 0; q < 4; q++)
-      for (int64_t c = 0; c < stride; c++) {
-        const size_t i = size_t(q) * stride + size_t(c);
-        if (c >= N || h_slot[i] < 0) h_nbv[i] = int(std::min<int64_t>(c, N - 1));
-        else h_nbv[i] = h_nb[i] >= 0 ? (h_nb[i] >> 2) : h_nb[i];
+    // node-based layout of the fast forms: a cell's vertices sorted by node
+    // id; face m is the face opposite vertex m
+    const bool fast = p.precision != NF_PREC_FP64_REF;
+    std::vector<int> h_cnode, h_gcode, h_nbvf, h_nbsf, hb_slotf;
+    if (fast) {
+      h_cnode.assign(size_t(4) * stride, 0);
+      h_gcode.assign(size_t(stride), 0);
+      h_nbvf.assign(size_t(4) * stride, 0);
+      h_nbsf.assign(size_t(4) * stride, 0);
+      for (int64_t c = 0; c < stride; c++)
+        for (int q = 0; q < 4; q++) h_nbvf[size_t(q) * stride + size_t(c)] = int(std::min<int64_t>(c, N - 1));
+      std::vector<uint32_t> sorted(size_t(4) * N);
+      for (int64_t c = 0; c < N; c++) {
+        uint32_t v[4] = {m.tet[size_t(4 * c)], m.tet[size_t(4 * c + 1)], m.tet[size_t(4 * c + 2)],
+                         m.tet[size_t(4 * c + 3)]};
+        std::sort(v, v + 4);
+        const int64_t d = m.dev_of_ref[size_t(c)];
+        for (int q = 0; q < 4; q++) {
+          sorted[size_t(4 * c + q)] = v[q];
+          h_cnode[size_t(q) * stride + size_t(d)] = int(v[q]);
+        }
       }
+      auto P = [&](uint32_t id, int e) { return m.nodes[size_t(3) * id + size_t(e)]; };
+      // index of the vertex of ref cell c that face f does not contain, and
+      // whether the normal from the ascending triple points into the cell
+      auto face_of = [&](int64_t c, int64_t f, int* mface, bool* inward) {
+        const uint32_t* fn = &m.face_nodes[size_t(3 * f)];
+        int om = -1;
+        for (int q = 0; q < 4; q++) {
+          const uint32_t v = sorted[size_t(4 * c + q)];
+          if (v != fn[0] && v != fn[1] && v != fn[2]) om = q;
+        }
+        if (om < 0) throw std::runtime_error("face nodes do not match its cell");
+        uint32_t t[3];
+        int k = 0;
+        for (int q = 0; q < 4; q++)
+          if (q != om) t[k++] = sorted[size_t(4 * c + q)];
+        double e1[3], e2[3], S[3], cen[3], fc[3];
+        for (int e = 0; e < 3; e++) {
+          e1[e] = P(t[1], e) - P(t[0], e);
+          e2[e] = P(t[2], e) - P(t[0], e);
+          fc[e] = (P(t[0], e) + P(t[1], e) + P(t[2], e)) / 3.0;
+          cen[e] = 0.25 * (P(sorted[size_t(4 * c)], e) + P(sorted[size_t(4 * c + 1)], e) +
+                           P(sorted[size_t(4 * c + 2)], e) + P(sorted[size_t(4 * c + 3)], e));
+        }
+        S[0] = e1[1] * e2[2] - e1[2] * e2[1];
+        S[1] = e1[2] * e2[0] - e1[0] * e2[2];
+        S[2] = e1[0] * e2[1] - e1[1] * e2[0];
+        const double dd = S[0] * (fc[0] - cen[0]) + S[1] * (fc[1] - cen[1]) + S[2] * (fc[2] - cen[2]);
+        *mface = om;
+        *inward = dd < 0.0;
+      };
+      hb_slotf.assign(size_t(nbf), 0);
+      std::vector<int> bindex(static_cast<size_t>(F), -1);  // boundary index of a device face
+      for (int b = 0; b < nbf; b++) bindex[size_t(bfaces[size_t(b)].face)] = b;
+      for (int64_t f = 0; f < F; f++) {
+        const int64_t ci = m.face_i[size_t(f)];
+        const int64_t di = m.dev_of_ref[size_t(ci)];
+        int mi;
+        bool ini;
+        face_of(ci, f, &mi, &ini);
+        int& gi = h_gcode[size_t(di)];
+        gi |= (1 | (ini ? 2 : 0)) << (3 * mi);  // owner side: bit 2 clear
+        const uint32_t j = m.face_j[size_t(f)];
+        if (j < uint32_t(N)) {
+          const int64_t dj = m.dev_of_ref[j];
+          int mj;
+          bool inj;
+          face_of(j, f, &mj, &inj);
+          h_gcode[size_t(dj)] |= (1 | (inj ? 2 : 0) | 4) << (3 * mj);
+          h_nbvf[size_t(mi) * stride + size_t(di)] = int(dj);
+          h_nbvf[size_t(mj) * stride + size_t(dj)] = int(di);
+          h_nbsf[size_t(mi) * stride + size_t(di)] = int(dj << 2) | mj;
+          h_nbsf[size_t(mj) * stride + size_t(dj)] = int(di << 2) | mi;
+        } else {
+          const int b = bindex[size_t(fdev[size_t(f)])];
+          h_nbvf[size_t(mi) * stride + size_t(di)] = -(1 + b);
+          h_nbsf[size_t(mi) * stride + size_t(di)] = -(1 + b);
+          hb_slotf[size_t(b)] = mi;
+        }
+      }
+    }
     s->nb = nbf;
     s->bstride = std::max(64, (nbf + 63) / 64 * 64);
-    std::vector<double> h_vol(size_t(stride), 1.0), h_dS(size_t(3) * stride, 0.0),
-        h_hv(size_t(stride), 0.5);
+    std::vector<double> h_vol(size_t(stride), 1.0), h_dS(size_t(3) * stride, 0.0);
     for (int64_t c = 0; c < N; c++) {
       const int64_t d = m.dev_of_ref[size_t(c)];
       h_vol[size_t(d)] = m.vol[size_t(c)];
-      h_hv[size_t(d)] = 0.5 / m.vol[size_t(c)];
       for (int k = 0; k < 3; k++) h_dS[size_t(k) * stride + size_t(d)] = m.dS[size_t(3 * c + k)];
     }
     // boundary conditions per patch
@@ -774,13 +842,26 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     s->b_face.upload(hb_face, st);
     s->b_patch.upload(hb_patch, st);
     s->rs.upload(h_rs, st);
-    s->sg.upload(h_sg, st);
-    s->nbv.upload(h_nbv, st);
+    if (fast) {
+      s->cnode.upload(h_cnode, st);
+      s->gcode.upload(h_gcode, st);
+      s->nbvf.upload(h_nbvf, st);
+      s->nbsf.upload(h_nbsf, st);
+      s->b_slotf.upload(hb_slotf, st);
+      std::vector<double> n4(size_t(4) * m.n_nodes, 0.0);
+      for (int64_t v = 0; v < m.n_nodes; v++)
+        for (int e = 0; e < 3; e++) n4[size_t(4 * v + e)] = m.nodes[size_t(3 * v + e)];
+      s->nodes4.upload(n4, st);
+      if (p.precision == NF_PREC_MIXED) {
+        std::vector<float> n4f(n4.size());
+        for (size_t i = 0; i < n4.size(); i++) n4f[i] = float(n4[i]);
+        s->nodes4_32.upload(n4f, st);
+      }
+    }
     s->S.upload(h_S, st);
     s->nhat.upload(h_n, st);
     s->area.upload(h_a, st);
     s->vol.upload(h_vol, st);
-    s->hvinv.upload(h_hv, st);
     s->dS.upload(h_dS, st);
     s->patches.upload(h_pb, st);
     if (p.precision == NF_PREC_MIXED) {
@@ -793,8 +874,6 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
       s->nhat32.upload(tof(h_n), st);
       s->area32.upload(tof(h_a), st);
       s->rs32.upload(tof(h_rs), st);
-      s->sg32.upload(tof(h_sg), st);
-      s->hvinv32.upload(tof(h_hv), st);
       s->vg32.alloc(size_t(5) * s->bstride);
       s->fb32.alloc(size_t(5) * s->bstride);
       s->vg32.zero(st);
