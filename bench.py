@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--block", type=int, default=0, help="fix the block size (no tuning)")
+    ap.add_argument("--variant", type=int, default=0, help="with --block: fast-kernel variant")
     return ap.parse_args()
 
 
@@ -134,22 +135,27 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, precision: str):
-    """Compulsory HBM bytes per launch of each kernel (every datum once).
+def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int, precision: str,
+                      local_dt: bool):
+    """Compulsory HBM bytes of one launch of each stage kernel (every datum the
+    kernel must read or write, once; neighbours' values are other cells' own
+    values and are not counted again). Fast forms (fp64, mixed):
 
-    flux_update, per cell: V, grad, phi of the cell (40+120+40), U of the stage
-    input (40), U^n (40, stages 2 and 3: 2/3 on average), vol (8), 4 slots (16),
-    writes U and V (80); per face: owner/neighbour ids (8), unit normal and
-    area (32), both centroid-to-face vectors (48).
-    gradient_limiter, per cell: V (40), vol (8), slots (16), writes grad and
-    phi (160); per face: ids (8), S (24), both r vectors (48), and the unit
-    normal of boundary faces (24).
+    gradient_node, per cell: V (5 r), 4 vertex ids (16), 4 neighbour ids (16),
+    face code (4), vol (8), writes 4 face states (20 r); plus the node array
+    (4 r per node) and one ghost state per boundary face (5 r).
+    flux_node, per cell: 4 own face states (20 r), 4 neighbour face ids (16),
+    face code (4), 4 vertex ids (16), U (40), U^n (40 at stages 2 and 3: 2/3
+    on average), vol (8), local dt (8 with local time stepping), writes U and
+    V (80, plus 20 for the FP32 copy in mixed precision) and R_rho/vol at the
+    first stage (8, 1/3 on average); plus the node array and one boundary flux
+    per boundary face (5 r).
+    r = 8 bytes (fp64) or 4 (mixed) for face work; U, V, vol, dt are FP64.
     """
     r = 4 if precision == "mixed" else 8
-    vcell = 5 * r + 15 * r + 5 * r
-    flux = n_cells * (vcell + 40 + 40 * 2 / 3 + 8 + 16 + 80 + (20 if precision == "mixed" else 0)) \
-        + n_faces * (8 + 4 * r + 6 * r)
-    grad = n_cells * (5 * r + 8 + 16 + 20 * r) + n_faces * (8 + 3 * r + 6 * r) + n_boundary * 3 * r
+    grad = n_cells * (5 * r + 16 + 16 + 4 + 8 + 20 * r) + n_nodes * 4 * r + n_boundary * 5 * r
+    flux = n_cells * (20 * r + 16 + 4 + 16 + 40 + 40 * 2 / 3 + 8 + (8 if local_dt else 0) + 80
+                      + (20 if precision == "mixed" else 0) + 8 / 3) + n_nodes * 4 * r + n_boundary * 5 * r
     return {"flux": flux, "gradient": grad}
 
 
@@ -257,7 +263,7 @@ def main():
     t_mesh = time.perf_counter() - t0
     cfg = S.Config(precision=args.precision, CFL=0.8, local_time_stepping=lts, density_fs=fs[0],
                    velocity_fs=list(fs[1:4]), pressure_fs=fs[4])
-    solver = S.EulerSolver(cfg, mesh, U0=U0, block_size=args.block)
+    solver = S.EulerSolver(cfg, mesh, U0=U0, block_size=args.block, variant=args.variant)
     lib = L.load()
     N = mesh.n_cells
 
@@ -292,7 +298,7 @@ def main():
             ((L.NF_KERNEL_TIMESTEP, "timestep"), (L.NF_KERNEL_GRADIENT, "gradient"), (L.NF_KERNEL_FLUX, "flux"),
              (L.NF_KERNEL_OTHER, "other"))}
     nb = mesh.n_ghost
-    ab = algorithmic_bytes(N, mesh.n_faces, nb, args.precision)
+    ab = algorithmic_bytes(N, mesh.n_faces, nb, int(mesh.info.n_nodes), args.precision, lts)
     hbm, hbm_kind = measured_peaks()
     dom = max(("flux", "gradient"), key=lambda k: kern[k][0] * kern[k][1])
     ach = ab[dom] / (kern[dom][0] * 1e-3) / 1e9

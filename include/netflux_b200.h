@@ -158,7 +158,9 @@ typedef struct {
   const nf_patch_bc* patches;
   int n_patches;
   double freestream[5]; /* Config::get_primvars_inf (rho,u,v,w,p) */
-  int block_size;       /* 0: tuned default */
+  int block_size;       /* 0: library default; > 0: fixed block size of the
+                           gradient and flux kernels (no tuning) */
+  int kernel_variant;   /* with block_size > 0: fast-kernel variant (see nf_tune) */
 } nf_params;
 
 void nf_params_default(nf_params* p);

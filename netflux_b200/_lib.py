@@ -52,7 +52,7 @@ class NfParams(C.Structure):
                 ("dt_from_current_state", C.c_int), ("keep_stage_fields", C.c_int),
                 ("cfl", C.c_double), ("t_end", C.c_double),
                 ("patches", C.POINTER(NfPatchBC)), ("n_patches", C.c_int),
-                ("freestream", C.c_double * 5), ("block_size", C.c_int)]
+                ("freestream", C.c_double * 5), ("block_size", C.c_int), ("kernel_variant", C.c_int)]
 
 
 class NetFluxError(RuntimeError):

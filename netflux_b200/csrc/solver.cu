@@ -649,6 +649,7 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     s->block = p.block_size > 0 ? p.block_size : 256;
     if (p.block_size > 0) {
       s->kgrad.block = s->kflux.block = std::min(p.block_size, 128);
+      s->kgrad.variant = s->kflux.variant = std::max(0, std::min(p.kernel_variant, 3));
       s->tuned = true;  // a caller-fixed shape is not tuned
     }
     if (s->block % 32 || s->block > 256) throw std::runtime_error("block_size must be a multiple of 32, <= 256");

@@ -205,7 +205,7 @@ class Mesh:
 
 def make_params(config: Config, mesh: Mesh, keep_stage_fields: bool = False,
                 patch_states: Optional[Sequence[Sequence[float]]] = None,
-                block_size: int = 0) -> "tuple[L.NfParams, object]":
+                block_size: int = 0, variant: int = 0) -> "tuple[L.NfParams, object]":
     """nf_params for ``config`` on ``mesh`` (the patch array is returned too, to keep it alive)."""
     p = L.NfParams()
     L.load().nf_params_default(C.byref(p))
@@ -219,6 +219,7 @@ def make_params(config: Config, mesh: Mesh, keep_stage_fields: bool = False,
     p.cfl = config.CFL
     p.t_end = config.t_end
     p.block_size = int(block_size)
+    p.kernel_variant = int(variant)
     for k in range(5):
         p.freestream[k] = config.primvars_inf[k]
     arr = None
@@ -264,10 +265,10 @@ class EulerSolver:
     """EulerSolver(config, grid): the device solver for one (possibly batched) mesh."""
 
     def __init__(self, config: Config, mesh: Mesh, U0: Optional[np.ndarray] = None,
-                 keep_stage_fields: bool = False, patch_states=None, block_size: int = 0):
+                 keep_stage_fields: bool = False, patch_states=None, block_size: int = 0, variant: int = 0):
         self.mesh = mesh
         self.n_cells = mesh.n_cells
-        params, self._patch_arr = make_params(config, mesh, keep_stage_fields, patch_states, block_size)
+        params, self._patch_arr = make_params(config, mesh, keep_stage_fields, patch_states, block_size, variant)
         self._h = L.load().nf_create(mesh._h, C.byref(params))
         if not self._h:
             raise L.NetFluxError(L.NF_ERR_ARG, L.last_error(None))
