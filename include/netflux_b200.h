@@ -161,6 +161,17 @@ typedef struct {
   int block_size;       /* 0: library default; > 0: fixed block size of the
                            gradient and flux kernels (no tuning) */
   int kernel_variant;   /* with block_size > 0: fast-kernel variant (see nf_tune) */
+  /* Limiter ratchet (extension; the reference's Barth limiter is always live,
+   * Numerics.hpp:148-250, and its residual stalls near a 1e-3 drop on steady
+   * problems). Once a case's ratchet is on, every stage's limiter value of a
+   * cell and variable is the minimum of the live value and the value kept so
+   * far, and is kept; it can only tighten, so it stops changing and the
+   * residual converges. It turns on for every case at step
+   * limiter_ratchet_step (> 0; steps counted from nf_set_state), and in
+   * nf_solve_steady for a case whose residual drop reaches
+   * limiter_ratchet_drop (> 0). Both 0: off. */
+  int64_t limiter_ratchet_step;
+  double limiter_ratchet_drop;
 } nf_params;
 
 void nf_params_default(nf_params* p);
@@ -178,6 +189,20 @@ int nf_step(nf_solver* s);
 /* n_steps x (calc_timestep + step) on the device; time (may be NULL) returns
  * the accumulated time. Uses a CUDA graph after the first call. */
 int nf_advance(nf_solver* s, int64_t n_steps, double* time_out);
+/* Steady solve with local time stepping (and the limiter ratchet of
+ * nf_params when set): run steps until every case's
+ * density residual (RMS of R_rho/vol over its cells, first stage of a step)
+ * is at most tol times its value at the first step, or until max_steps. The
+ * residuals are checked every check_every steps (CUDA graph replays in
+ * between); a converged case is frozen (its cells keep their state exactly)
+ * while the others continue. Per case (arrays of n_cases, any may be NULL):
+ * steps to convergence (minus the steps run if it did not converge), the
+ * first and last residual, and the device time until it converged. The
+ * reference has no steady driver (it runs n_timesteps global steps,
+ * Driver.cpp:31-57). */
+int nf_solve_steady(nf_solver* s, double tol, int64_t max_steps, int check_every, int64_t* steps_per_case,
+                    double* res0_per_case, double* res_per_case, double* ms_per_case);
+
 /* Density residual of the first stage of the last step: RMS and max of
  * R_rho,i / vol_i over all cells (per case: n_cases pairs). */
 int nf_get_residual(nf_solver* s, double* rms_and_max, int n_cases);

@@ -30,7 +30,7 @@ EXPORTED = (
     "nf_mesh_export", "nf_mesh_get_permutation", "nf_mesh_get_case_offsets", "nf_mesh_destroy",
     "nf_params_default", "nf_create", "nf_set_state", "nf_get_state", "nf_calc_timestep", "nf_set_timestep",
     "nf_step", "nf_advance", "nf_get_residual", "nf_get_field", "nf_synchronize", "nf_last_error", "nf_destroy",
-    "nf_time_steps", "nf_residual_norms_noalloc", "nf_tune",
+    "nf_time_steps", "nf_residual_norms_noalloc", "nf_tune", "nf_solve_steady",
 )
 NF_KERNEL_TIMESTEP, NF_KERNEL_GRADIENT, NF_KERNEL_FLUX, NF_KERNEL_OTHER, NF_KERNEL_COUNT = range(5)
 
@@ -52,7 +52,8 @@ class NfParams(C.Structure):
                 ("dt_from_current_state", C.c_int), ("keep_stage_fields", C.c_int),
                 ("cfl", C.c_double), ("t_end", C.c_double),
                 ("patches", C.POINTER(NfPatchBC)), ("n_patches", C.c_int),
-                ("freestream", C.c_double * 5), ("block_size", C.c_int), ("kernel_variant", C.c_int)]
+                ("freestream", C.c_double * 5), ("block_size", C.c_int), ("kernel_variant", C.c_int),
+                ("limiter_ratchet_step", C.c_int64), ("limiter_ratchet_drop", C.c_double)]
 
 
 class NetFluxError(RuntimeError):
@@ -100,6 +101,7 @@ def load() -> C.CDLL:
         "nf_time_steps": (I, [P, I64, I, dp, dp, i64p]),
         "nf_residual_norms_noalloc": (I, [P, I64, P, P]),
         "nf_tune": (I, [P, C.POINTER(C.c_int)]),
+        "nf_solve_steady": (I, [P, D, I64, I, i64p, dp, dp, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -72,6 +72,7 @@ struct StageArgs {
   int scheme;            // 0 explicit Euler, 1 TVD-RK3
   int stage;             // 0, 1, 2
   int local_dt;
+  int freeze;            // a cell with dt == 0 keeps its state exactly (converged case)
   const double* Vin;     // primitives of the stage input [5][stride]
   double* fs;            // reconstructed face states [4 slots][5][stride]
   double* grad;          // optional copy of the gradient [15][stride] (k*3+d)
@@ -96,7 +97,29 @@ struct StageArgs {
   double* fb;
   float* vg32;
   float* fb32;
+  // limiter ratchet (extension): per-cell case, per-case switch (null: off)
+  // and the kept limiter values [5][stride] (FP64 or FP32 with the state form)
+  const int* cell_case;
+  const int* lim_ratchet;
+  double* phi_keep;
+  float* phi_keep32;
 };
+
+// Once a case's ratchet is on, a cell's limiter value is the minimum of the
+// live value and the kept one, and is kept: it only tightens, so it settles
+// and the steady residual can converge (the live Barth limiter makes it stall).
+__device__ __forceinline__ bool ratchet_on(const StageArgs& a, int c) {
+  return a.lim_ratchet != nullptr && a.lim_ratchet[a.cell_case[c]] != 0;
+}
+template <typename T>
+__device__ __forceinline__ T ratchet(const StageArgs& a, size_t at, T phi) {
+  T* keep;
+  if constexpr (sizeof(T) == 8) keep = a.phi_keep;
+  else keep = a.phi_keep32;
+  const T v = (keep[at] < phi) ? keep[at] : phi;  // std::min(phi, kept)
+  keep[at] = v;
+  return v;
+}
 
 enum : int { kScalDtMin = 0, kScalTime = 1, kScalTEnd = 2, kScalDtUsed = 3, kScalCount = 8 };
 
@@ -249,6 +272,7 @@ __global__ void __launch_bounds__(256) gradient_limiter_kernel(MeshView<T> m, St
       }
       phi = rmin(phi, fc);
     }
+    if (ratchet_on(a, c)) phi = ratchet(a, size_t(k) * st + c, phi);
   }
 #pragma unroll
   for (int q = 0; q < 4; q++) {
@@ -369,6 +393,10 @@ __global__ void __launch_bounds__(256) flux_update_kernel(MeshView<T> m, StageAr
     const double qf = 2.0 / 3.0 * dt / vol;
 #pragma unroll
     for (int k = 0; k < 5; k++) Unew[k] = 1.0 / 3.0 * Uo[k] + 2.0 / 3.0 * U[k] + qf * R[k];
+  }
+  if (a.freeze && dt == 0.0) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) Unew[k] = U[k];
   }
   double Vn[5];
   cons_to_prim<double, kRef>(Unew, Vn);
@@ -496,6 +524,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
   const T ssum[3] = {(S[0][0] + S[1][0]) + (S[2][0] + S[3][0]), (S[0][1] + S[1][1]) + (S[2][1] + S[3][1]),
                      (S[0][2] + S[1][2]) + (S[2][2] + S[3][2])};
   const T hv = T(0.5 / m.vol[c]);
+  const bool rat = a.barth && ratchet_on(a, c);
 #pragma unroll 1
   for (int k = 0; k < 5; k++) {
     T vc, vo[4];
@@ -533,6 +562,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
         Dn = better ? D : Dn;
       }
       phi = An / Dn;
+      if (rat) phi = ratchet(a, size_t(k) * st + c, phi);
     }
 #pragma unroll
     for (int q = 0; q < 4; q++) fs[(q * 5 + k) * st + c] = fma(phi, gr[q], vc);
@@ -659,6 +689,10 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
 #pragma unroll
     for (int k = 0; k < 5; k++) Unew[k] = 1.0 / 3.0 * a.Un[k * st + c] + 2.0 / 3.0 * a.Uin[k * st + c] + qf * R[k];
   }
+  if (a.freeze && dt == 0.0) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) Unew[k] = a.Uin[k * st + c];
+  }
   double Vn[5];
   cons_to_prim<double, false>(Unew, Vn);
   bool finite = true;
@@ -748,6 +782,8 @@ struct DtArgs {
   double* dt_local;  // per-cell dt, or nullptr
   unsigned long long* dt_min_bits;
   unsigned* status;
+  const int* cell_case;    // case of each cell (batched meshes)
+  const int* case_frozen;  // nonzero: the case has converged; its cells get dt = 0
 };
 
 template <bool kRef>
@@ -762,9 +798,12 @@ __global__ void __launch_bounds__(256) timestep_kernel(MeshView<double> m, DtArg
     const double sy = (fabs(V2) + cs) * m.dS[st + c];
     const double sz = (fabs(V3) + cs) * m.dS[2 * st + c];
     const double d = a.cfl * m.vol[c] / (sx + sy + sz);
-    if (a.dt_local) a.dt_local[c] = d;
-    if (!(d > 0.0) && !isnan(d)) atomicOr(a.status, kErrDt);
-    if (d > 0.0) dtc = d;  // std::min skips NaN (comparisons with NaN are false)
+    const bool frozen = a.case_frozen && a.case_frozen[a.cell_case[c]];
+    if (a.dt_local) a.dt_local[c] = frozen ? 0.0 : d;
+    if (!frozen) {
+      if (!(d > 0.0) && !isnan(d)) atomicOr(a.status, kErrDt);
+      if (d > 0.0) dtc = d;  // std::min skips NaN (comparisons with NaN are false)
+    }
   }
   // warp then block minimum, one atomic per block
 #pragma unroll

@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <numeric>
 #include <string>
@@ -172,6 +173,15 @@ struct nf_solver {
   DevBuf<unsigned> status;
   DevBuf<long long> chunk_begin, chunk_end, case_cells;
   DevBuf<int> case_chunk0;
+  DevBuf<int> cell_case, case_frozen;  // per-cell case; per-case convergence freeze
+  bool freeze = false;
+  // limiter ratchet (extension): per-case switch and the kept limiter values
+  bool ratchet_alloc = false, ratchet_step_done = false;
+  int64_t steps_done = 0;  // steps since nf_set_state
+  DevBuf<int> case_ratchet;
+  DevBuf<double> phi_keep;
+  DevBuf<float> phi_keep32;
+  std::vector<int> h_ratchet;
   int n_chunks = 0;
   double* h_scal = nullptr;  // pinned
   int vcur = 0;              // V buffer holding the primitives of the current state
@@ -238,9 +248,76 @@ struct nf_solver {
     a.dt_local = p.local_time_stepping ? dt_local.p : nullptr;
     a.dt_min_bits = reinterpret_cast<unsigned long long*>(scal.p + nf::kScalDtMin);
     a.status = status.p;
+    a.cell_case = cell_case.p;
+    a.case_frozen = freeze ? case_frozen.p : nullptr;
     prof_begin(NF_KERNEL_TIMESTEP);
     nf::launch_timestep(view64(), a, launch());
     prof_end();
+  }
+
+  void ratchet_reset() {
+    ratchet_step_done = false;
+    if (!ratchet_alloc) return;
+    std::fill(h_ratchet.begin(), h_ratchet.end(), 0);
+    ck(cudaMemsetAsync(case_ratchet.p, 0, size_t(n_cases) * sizeof(int), stream), "ratchet reset");
+    // bytes 0x7f: a value above every limiter value (<= 1) in FP64 and FP32
+    if (phi_keep.p) ck(cudaMemsetAsync(phi_keep.p, 0x7f, size_t(5) * stride * sizeof(double), stream), "ratchet reset");
+    if (phi_keep32.p)
+      ck(cudaMemsetAsync(phi_keep32.p, 0x7f, size_t(5) * stride * sizeof(float), stream), "ratchet reset");
+  }
+  void ratchet_start(int cs) {  // cs < 0: every case
+    if (!ratchet_alloc) return;
+    for (int k = 0; k < n_cases; k++)
+      if (cs < 0 || k == cs) h_ratchet[size_t(k)] = 1;
+    // pageable source: the call returns once the values are staged
+    ck(cudaMemcpyAsync(case_ratchet.p, h_ratchet.data(), size_t(n_cases) * sizeof(int), cudaMemcpyHostToDevice,
+                       stream),
+       "ratchet H2D");
+  }
+  // steps before the ratchet's start step, or all of n once it has started
+  int64_t ratchet_due(int64_t n) {
+    if (!ratchet_alloc || p.limiter_ratchet_step <= 0 || ratchet_step_done) return n;
+    if (steps_done >= p.limiter_ratchet_step) {
+      ratchet_start(-1);
+      ratchet_step_done = true;
+      return n;
+    }
+    return std::min<int64_t>(n, p.limiter_ratchet_step - steps_done);
+  }
+
+  // n x (calc_timestep + step), replays of a two-step CUDA graph where
+  // possible; the ratchet starts at its step.
+  void run_steps(int64_t n) {
+    while (n > 0) {
+      int64_t left = ratchet_due(n);
+      n -= left;
+      steps_done += left;
+      if (left >= 2 && stepped) {
+        const int v0 = vcur;
+        if (!graph[v0]) {
+          // capture two steps: the V buffers return to their roles afterwards
+          cudaGraph_t g = nullptr;
+          ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+          for (int k = 0; k < 2; k++) {
+            enqueue_dt();
+            enqueue_step();
+          }
+          ck(cudaStreamEndCapture(stream, &g), "end capture");
+          ck(cudaGraphInstantiate(&graph[v0], g, 0), "graph instantiate");
+          cudaGraphDestroy(g);
+          vcur = v0;
+        }
+        while (left >= 2) {
+          ck(cudaGraphLaunch(graph[v0], stream), "graph launch");
+          left -= 2;
+        }
+      }
+      while (left > 0) {
+        enqueue_dt();
+        enqueue_step();
+        left--;
+      }
+    }
   }
 
   void launch_gradient(const nf::StageArgs& a, const KCfg& k) {
@@ -366,6 +443,7 @@ struct nf_solver {
       a.scheme = p.time_scheme == NF_TVD_RK3 ? 1 : 0;
       a.stage = s;
       a.local_dt = p.local_time_stepping;
+      a.freeze = freeze && p.local_time_stepping;
       a.Vin = Vbuf(vcur);
       a.Vout = Vbuf(1 - vcur);
       a.fs = fs.p;
@@ -380,6 +458,12 @@ struct nf_solver {
       a.dt_local = dt_local.p;
       a.scal = scal.p;
       a.status = status.p;
+      if (ratchet_alloc) {
+        a.cell_case = cell_case.p;
+        a.lim_ratchet = case_ratchet.p;
+        a.phi_keep = phi_keep.p;
+        a.phi_keep32 = phi_keep32.p;
+      }
       if (a.scheme == 0) {
         a.Uin = U.p;
         a.Uout = U.p;
@@ -944,6 +1028,23 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     s->case_cells.upload(cc, st);
     s->case_chunk0.upload(c0, st);
     s->part.alloc(size_t(2) * s->n_chunks);
+    {
+      std::vector<int> cc2(static_cast<size_t>(stride), 0);
+      for (int cs = 0; cs < s->n_cases; cs++)
+        for (int64_t c = m.case_offsets[size_t(cs)]; c < m.case_offsets[size_t(cs + 1)]; c++) cc2[size_t(c)] = cs;
+      s->cell_case.upload(cc2, st);
+      s->case_frozen.alloc(size_t(s->n_cases));
+      s->case_frozen.zero(st);
+    }
+    if (p.spatial_order == NF_SECOND_ORDER && p.limiter == NF_LIMITER_BARTH &&
+        (p.limiter_ratchet_step > 0 || p.limiter_ratchet_drop > 0.0)) {
+      s->ratchet_alloc = true;
+      s->case_ratchet.alloc(size_t(s->n_cases));
+      s->h_ratchet.assign(size_t(s->n_cases), 0);
+      if (p.precision == NF_PREC_MIXED) s->phi_keep32.alloc(size_t(5) * stride);
+      else s->phi_keep.alloc(size_t(5) * stride);
+      s->ratchet_reset();
+    }
     s->stage.alloc(size_t(5) * N);
     {
       std::vector<long long> dor(m.dev_of_ref.begin(), m.dev_of_ref.end());
@@ -984,6 +1085,8 @@ int nf_set_state(nf_solver* s, const double* U, int64_t n_cells) {
     }
     s->vcur = 0;
     s->stepped = false;
+    s->steps_done = 0;
+    s->ratchet_reset();
     ck(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream), "status reset");
     ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
     ck(cudaGetLastError(), "nf_set_state");
@@ -1042,7 +1145,9 @@ int nf_set_timestep(nf_solver* s, double dt) {
 
 int nf_step(nf_solver* s) {
   return guarded(s, [&]() -> int {
+    s->ratchet_due(1);
     s->enqueue_step();
+    s->steps_done++;
     ck(cudaGetLastError(), "step launch");
     return NF_OK;
   });
@@ -1051,32 +1156,7 @@ int nf_step(nf_solver* s) {
 int nf_advance(nf_solver* s, int64_t n_steps, double* time_out) {
   return guarded(s, [&]() -> int {
     if (n_steps < 0) return NF_ERR_ARG;
-    int64_t left = n_steps;
-    if (left >= 2 && s->stepped) {
-      const int v0 = s->vcur;
-      if (!s->graph[v0]) {
-        // capture two steps: the V buffers return to their roles afterwards
-        cudaGraph_t g = nullptr;
-        ck(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-        for (int k = 0; k < 2; k++) {
-          s->enqueue_dt();
-          s->enqueue_step();
-        }
-        ck(cudaStreamEndCapture(s->stream, &g), "end capture");
-        ck(cudaGraphInstantiate(&s->graph[v0], g, 0), "graph instantiate");
-        cudaGraphDestroy(g);
-        s->vcur = v0;
-      }
-      while (left >= 2) {
-        ck(cudaGraphLaunch(s->graph[v0], s->stream), "graph launch");
-        left -= 2;
-      }
-    }
-    while (left > 0) {
-      s->enqueue_dt();
-      s->enqueue_step();
-      left--;
-    }
+    s->run_steps(n_steps);
     ck(cudaGetLastError(), "advance launch");
     int rc = s->check_status();
     if (time_out) {
@@ -1087,17 +1167,125 @@ int nf_advance(nf_solver* s, int64_t n_steps, double* time_out) {
   });
 }
 
+static void enqueue_residual(nf_solver* s) {
+  residual_partials_kernel<<<s->n_chunks, 256, 0, s->stream>>>(s->res_cell.p, s->chunk_begin.p, s->chunk_end.p,
+                                                               s->part.p);
+  residual_finalize_kernel<<<(s->n_cases + 127) / 128, 128, 0, s->stream>>>(s->part.p, s->case_chunk0.p,
+                                                                          s->case_cells.p, s->n_cases,
+                                                                          s->res_out.p);
+}
+
+int nf_solve_steady(nf_solver* s, double tol, int64_t max_steps, int check_every, int64_t* steps_per_case,
+                    double* res0_per_case, double* res_per_case, double* ms_per_case) {
+  return guarded(s, [&]() -> int {
+    if (!s->p.local_time_stepping) {
+      s->err = "nf_solve_steady needs local time stepping";
+      return NF_ERR_ARG;
+    }
+    if (!(tol > 0.0) || max_steps < 1 || check_every < 1) return NF_ERR_ARG;
+    const int nc = s->n_cases;
+    std::vector<int> frozen(size_t(nc), 0);
+    std::vector<int64_t> steps(size_t(nc), -1);
+    std::vector<double> r0(size_t(nc), 0.0), rl(size_t(nc), 0.0), ms(size_t(nc), 0.0), h(size_t(2) * nc);
+    // Graphs bake the freeze argument into their launches, so they are dropped
+    // when it is switched on and again when it is switched off; the guard
+    // restores the unfrozen solver on every exit, error paths included.
+    auto drop_graphs = [s]() {
+      for (auto& g : s->graph)
+        if (g) {
+          cudaGraphExecDestroy(g);
+          g = nullptr;
+        }
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    struct Restore {
+      nf_solver* s;
+      int nc;
+      cudaEvent_t *e0, *e1;
+      std::function<void()> drop;
+      ~Restore() {
+        if (*e0) cudaEventDestroy(*e0);
+        if (*e1) cudaEventDestroy(*e1);
+        s->freeze = false;
+        drop();
+        cudaMemsetAsync(s->case_frozen.p, 0, size_t(nc) * sizeof(int), s->stream);
+      }
+    } restore{s, nc, &e0, &e1, drop_graphs};
+    ck(cudaMemsetAsync(s->case_frozen.p, 0, size_t(nc) * sizeof(int), s->stream), "freeze reset");
+    s->freeze = true;
+    drop_graphs();
+    ck(cudaEventCreate(&e0), "cudaEventCreate");
+    ck(cudaEventCreate(&e1), "cudaEventCreate");
+    ck(cudaEventRecord(e0, s->stream), "cudaEventRecord");
+    auto read_res = [&]() {
+      enqueue_residual(s);
+      ck(cudaMemcpyAsync(h.data(), s->res_out.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
+         "residual D2H");
+      ck(cudaEventRecord(e1, s->stream), "cudaEventRecord");
+      ck(cudaEventSynchronize(e1), "cudaEventSynchronize");
+    };
+    // first step: the reference residual of every case
+    s->run_steps(1);
+    read_res();
+    int64_t done = 1, left = nc;
+    for (int cs = 0; cs < nc; cs++) {
+      r0[size_t(cs)] = h[size_t(2 * cs)];
+      rl[size_t(cs)] = r0[size_t(cs)];
+      if (!(r0[size_t(cs)] > 0.0)) {  // already steady
+        steps[size_t(cs)] = 1;
+        frozen[size_t(cs)] = 1;
+        left--;
+      }
+    }
+    while (left > 0 && done < max_steps) {
+      const int64_t k = std::min<int64_t>(check_every, max_steps - done);
+      ck(cudaMemcpyAsync(s->case_frozen.p, frozen.data(), size_t(nc) * sizeof(int), cudaMemcpyHostToDevice,
+                         s->stream),
+         "freeze H2D");
+      s->run_steps(k);
+      done += k;
+      read_res();
+      float t = 0.f;
+      ck(cudaEventElapsedTime(&t, e0, e1), "cudaEventElapsedTime");
+      for (int cs = 0; cs < nc; cs++) {
+        if (frozen[size_t(cs)]) continue;
+        rl[size_t(cs)] = h[size_t(2 * cs)];
+        if (!std::isfinite(rl[size_t(cs)])) {
+          s->err = "residual is not finite";
+          return NF_ERR_NONPHYSICAL;
+        }
+        if (s->ratchet_alloc && s->p.limiter_ratchet_drop > 0.0 && !s->h_ratchet[size_t(cs)] &&
+            rl[size_t(cs)] <= s->p.limiter_ratchet_drop * r0[size_t(cs)])
+          s->ratchet_start(cs);
+        if (rl[size_t(cs)] <= tol * r0[size_t(cs)]) {
+          frozen[size_t(cs)] = 1;
+          steps[size_t(cs)] = done;
+          ms[size_t(cs)] = t;
+          left--;
+        }
+      }
+    }
+    float t = 0.f;
+    ck(cudaEventElapsedTime(&t, e0, e1), "cudaEventElapsedTime");
+    for (int cs = 0; cs < nc; cs++)
+      if (steps[size_t(cs)] < 0) ms[size_t(cs)] = t;  // not converged: report the time spent
+    for (int cs = 0; cs < nc; cs++) {
+      if (steps_per_case) steps_per_case[cs] = steps[size_t(cs)] < 0 ? -done : steps[size_t(cs)];
+      if (res0_per_case) res0_per_case[cs] = r0[size_t(cs)];
+      if (res_per_case) res_per_case[cs] = rl[size_t(cs)];
+      if (ms_per_case) ms_per_case[cs] = ms[size_t(cs)];
+    }
+    return s->check_status();
+  });
+}
+
 int nf_get_residual(nf_solver* s, double* out, int n_cases) {
   return guarded(s, [&]() -> int {
     if (!out || n_cases != s->n_cases) {
       s->err = "nf_get_residual: n_cases does not match the mesh";
       return NF_ERR_ARG;
     }
-    residual_partials_kernel<<<s->n_chunks, 256, 0, s->stream>>>(s->res_cell.p, s->chunk_begin.p, s->chunk_end.p,
-                                                                 s->part.p);
-    residual_finalize_kernel<<<(s->n_cases + 127) / 128, 128, 0, s->stream>>>(s->part.p, s->case_chunk0.p,
-                                                                            s->case_cells.p, s->n_cases,
-                                                                            s->res_out.p);
+    enqueue_residual(s);
     ck(cudaGetLastError(), "residual launch");
     std::vector<double> h(size_t(2) * s->n_cases);
     ck(cudaMemcpyAsync(h.data(), s->res_out.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
@@ -1199,6 +1387,7 @@ int nf_time_steps(nf_solver* s, int64_t n_steps, int per_kernel, double* ms_tota
       s->enqueue_step();
       left--;
     }
+    s->steps_done += n_steps;  // timing runs count as steps but do not start the ratchet
     ck(cudaEventRecord(e1, s->stream), "cudaEventRecord");
     ck(cudaEventSynchronize(e1), "cudaEventSynchronize");
     float ms = 0.f;

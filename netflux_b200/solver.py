@@ -94,6 +94,9 @@ class Config:
         self.local_time_stepping = bool(opts.get("local_time_stepping", False))
         self.t_end = float(opts.get("t_end", 0.0))
         self.patch_farfield: Dict[str, Sequence[float]] = dict(opts.get("patch_farfield", {}))
+        # limiter ratchet: from this step on / once a case's residual drop reaches this value
+        self.limiter_ratchet_step = int(opts.get("limiter_ratchet_step", 0))
+        self.limiter_ratchet_drop = float(opts.get("limiter_ratchet_drop", 0.0))
         self.delta_time = 0.0
         self.time = 0.0
         self.timestep = 0
@@ -220,6 +223,8 @@ def make_params(config: Config, mesh: Mesh, keep_stage_fields: bool = False,
     p.t_end = config.t_end
     p.block_size = int(block_size)
     p.kernel_variant = int(variant)
+    p.limiter_ratchet_step = config.limiter_ratchet_step
+    p.limiter_ratchet_drop = config.limiter_ratchet_drop
     for k in range(5):
         p.freestream[k] = config.primvars_inf[k]
     arr = None
@@ -267,6 +272,7 @@ class EulerSolver:
     def __init__(self, config: Config, mesh: Mesh, U0: Optional[np.ndarray] = None,
                  keep_stage_fields: bool = False, patch_states=None, block_size: int = 0, variant: int = 0):
         self.mesh = mesh
+        self.config = config
         self.n_cells = mesh.n_cells
         params, self._patch_arr = make_params(config, mesh, keep_stage_fields, patch_states, block_size, variant)
         self._h = L.load().nf_create(mesh._h, C.byref(params))
@@ -308,6 +314,16 @@ class EulerSolver:
         cfg = (C.c_int * 4)()
         _check(L.load().nf_tune(self._h, cfg), self._h)
         return {"gradient": {"block": cfg[0], "variant": cfg[1]}, "flux": {"block": cfg[2], "variant": cfg[3]}}
+
+    def solve_steady(self, tol: float = 1e-6, max_steps: int = 100000, check_every: int = 50) -> dict:
+        """Local-time-stepping steady solve to a relative density-residual drop of ``tol`` (per case)."""
+        nc = self.mesh.n_cases
+        steps = np.zeros(nc, np.int64)
+        r0, r1, ms = np.zeros(nc), np.zeros(nc), np.zeros(nc)
+        _check(L.load().nf_solve_steady(self._h, float(tol), int(max_steps), int(check_every), L.i64ptr(steps),
+                                         L.dptr(r0), L.dptr(r1), L.dptr(ms)), self._h)
+        # the library returns -(steps run) for a case that did not reach tol
+        return {"steps": np.abs(steps), "converged": steps > 0, "res0": r0, "res": r1, "ms": ms}
 
     def synchronize(self) -> None:
         _check(L.load().nf_synchronize(self._h), self._h)

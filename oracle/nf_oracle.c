@@ -122,6 +122,8 @@ typedef struct {
   int64_t NC, NT, NF, NIF;
   double *V, *G, *L, *Vmax, *Vmin, *R;
   int* face_patch;
+  int ratchet; /* limiter-ratchet extension: phi = min(live phi, Lf), kept in Lf */
+  double* Lf;   /* starts at DBL_MAX */
 } work_t;
 
 /* Solver::evaluate_flux_balance (Solver.cpp:54-81) and what it calls. */
@@ -188,6 +190,8 @@ static void flux_balance(const nfo_mesh* m, const nfo_params* p, work_t* w, cons
           }
         }
       }
+      if (w->ratchet)
+        for (int64_t x = 0; x < 5 * NC; x++) w->Lf[x] = w->L[x] = dmin(w->L[x], w->Lf[x]);
     } else {
       for (int64_t x = 0; x < 5 * NC; x++) w->L[x] = 1.0; /* SolverData.cpp:331 */
     }
@@ -259,6 +263,10 @@ int nfo_run(const nfo_mesh* m, const nfo_params* p, double* U, int64_t n_steps, 
   w.Vmin = (double*)calloc((size_t)(5 * w.NC), sizeof(double));
   w.R = (double*)calloc((size_t)(5 * w.NC), sizeof(double));
   w.face_patch = (int*)calloc((size_t)w.NF, sizeof(int));
+  w.ratchet = 0;
+  w.Lf = p->limiter_ratchet_step > 0 ? (double*)malloc(sizeof(double) * 5 * w.NC) : NULL;
+  if (w.Lf)
+    for (int64_t x = 0; x < 5 * w.NC; x++) w.Lf[x] = DBL_MAX;
   double* Un = (double*)malloc(sizeof(double) * 5 * w.NC);
   double* dtl = p->local_time_stepping ? (double*)malloc(sizeof(double) * w.NC) : NULL;
   double* Vdt = (double*)malloc(sizeof(double) * 5 * w.NC);
@@ -266,7 +274,7 @@ int nfo_run(const nfo_mesh* m, const nfo_params* p, double* U, int64_t n_steps, 
   double time = 0.0;
   const int n_stages = p->time_scheme == 1 ? 3 : 1;
   if (!w.V || !w.G || !w.L || !w.Vmax || !w.Vmin || !w.R || !w.face_patch || !Un || !Vdt ||
-      (p->local_time_stepping && !dtl)) {
+      (p->local_time_stepping && !dtl) || (p->limiter_ratchet_step > 0 && !w.Lf)) {
     rc = 2;
     goto done;
   }
@@ -292,6 +300,7 @@ int nfo_run(const nfo_mesh* m, const nfo_params* p, double* U, int64_t n_steps, 
     }
     if (dt_hist) dt_hist[n] = dt;
     for (int s = 0; s < n_stages; s++) {
+      w.ratchet = p->limiter_ratchet_step > 0 && n >= p->limiter_ratchet_step;
       flux_balance(m, p, &w, U);
       if (s == 0 && res_out) {
         double ss = 0.0, mx = 0.0;
@@ -333,6 +342,7 @@ done:
   free(w.Vmin);
   free(w.R);
   free(w.face_patch);
+  free(w.Lf);
   free(Un);
   free(dtl);
   free(Vdt);

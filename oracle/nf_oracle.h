@@ -44,6 +44,9 @@ typedef struct {
   int dt_from_current_state; /* extension: dt from V(U^n) instead of the last stage's primitives */
   double cfl;
   double t_end;              /* extension: > 0 clips dt at t_end */
+  int64_t limiter_ratchet_step; /* extension: > 0 ratchets the Barth limiter from that step on (0-based):
+                                   every stage takes the minimum of its live value and the value
+                                   it kept, and keeps that; 0 keeps the limiter live */
 } nfo_params;
 
 /* Advance U (AoS [n_cells][5], in/out) by n_steps of calc_timestep + step.
