@@ -594,6 +594,45 @@ struct FaceIn {
   int kind;    // 0 no face, 1 interior (owner), 2 interior (neighbour side), 3 boundary
 };
 
+// Stage update of one cell from its flux balance R (TVD_RK3 Solver.cpp:103-133,
+// explicit_euler 83-101) in FP64, then the primitives of the new state
+// (set_primvars, SolverData.cpp:37-48), the optional dumps and the status.
+__device__ __forceinline__ void stage_update(const StageArgs& a, int c, int st, const double R[5], double vol) {
+  const double dt = a.local_dt ? a.dt_local[c] : stage_dt(a.scal);
+  double Unew[5];
+  if (a.scheme == 0 || a.stage == 0) {
+    const double qf = dt / vol;
+#pragma unroll
+    for (int k = 0; k < 5; k++) Unew[k] = fma(qf, R[k], a.Uin[k * st + c]);
+  } else if (a.stage == 1) {
+    const double qf = 0.25 * dt / vol;
+#pragma unroll
+    for (int k = 0; k < 5; k++) Unew[k] = 0.75 * a.Un[k * st + c] + 0.25 * a.Uin[k * st + c] + qf * R[k];
+  } else {
+    const double qf = 2.0 / 3.0 * dt / vol;
+#pragma unroll
+    for (int k = 0; k < 5; k++) Unew[k] = 1.0 / 3.0 * a.Un[k * st + c] + 2.0 / 3.0 * a.Uin[k * st + c] + qf * R[k];
+  }
+  if (a.freeze && dt == 0.0) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) Unew[k] = a.Uin[k * st + c];
+  }
+  double Vn[5];
+  cons_to_prim<double, false>(Unew, Vn);
+  bool finite = true;
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    a.Uout[k * st + c] = Unew[k];
+    a.Vout[k * st + c] = Vn[k];
+    if (a.Vout32) a.Vout32[k * st + c] = float(Vn[k]);
+    if (a.R) a.R[k * st + c] = R[k];
+    finite = finite && isfinite(R[k]) && isfinite(Unew[k]);
+  }
+  if (a.res_cell) a.res_cell[c] = R[0] / vol;
+  if (!finite) atomicOr(a.status, kErrNonFinite);
+  else if (!(Vn[0] > 0.0) || !(Vn[4] > 0.0)) atomicOr(a.status, kErrNonPhysical);
+}
+
 template <typename T, bool kPipe, int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -673,40 +712,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
       for (int k = 0; k < 5; k++) R[k] = own ? R[k] - double(Fl[k]) : R[k] + double(Fl[k]);
     }
   }
-  const double vol = m.vol[c];
-  const double dt = a.local_dt ? a.dt_local[c] : stage_dt(a.scal);
-  double Unew[5];
-  if (a.scheme == 0 || a.stage == 0) {
-    const double qf = dt / vol;
-#pragma unroll
-    for (int k = 0; k < 5; k++) Unew[k] = fma(qf, R[k], a.Uin[k * st + c]);
-  } else if (a.stage == 1) {
-    const double qf = 0.25 * dt / vol;
-#pragma unroll
-    for (int k = 0; k < 5; k++) Unew[k] = 0.75 * a.Un[k * st + c] + 0.25 * a.Uin[k * st + c] + qf * R[k];
-  } else {
-    const double qf = 2.0 / 3.0 * dt / vol;
-#pragma unroll
-    for (int k = 0; k < 5; k++) Unew[k] = 1.0 / 3.0 * a.Un[k * st + c] + 2.0 / 3.0 * a.Uin[k * st + c] + qf * R[k];
-  }
-  if (a.freeze && dt == 0.0) {
-#pragma unroll
-    for (int k = 0; k < 5; k++) Unew[k] = a.Uin[k * st + c];
-  }
-  double Vn[5];
-  cons_to_prim<double, false>(Unew, Vn);
-  bool finite = true;
-#pragma unroll
-  for (int k = 0; k < 5; k++) {
-    a.Uout[k * st + c] = Unew[k];
-    a.Vout[k * st + c] = Vn[k];
-    if (a.Vout32) a.Vout32[k * st + c] = float(Vn[k]);
-    if (a.R) a.R[k * st + c] = R[k];
-    finite = finite && isfinite(R[k]) && isfinite(Unew[k]);
-  }
-  if (a.res_cell) a.res_cell[c] = R[0] / vol;
-  if (!finite) atomicOr(a.status, kErrNonFinite);
-  else if (!(Vn[0] > 0.0) || !(Vn[4] > 0.0)) atomicOr(a.status, kErrNonPhysical);
+  stage_update(a, c, st, R, m.vol[c]);
 }
 
 // ---------------------------------------------------------------------------

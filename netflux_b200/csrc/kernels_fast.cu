@@ -1,5 +1,7 @@
 // Kernels with reciprocals and fused multiply-adds (FP64), and the
-// mixed-precision form (FP32 face work, FP64 state and update).
+// mixed-precision form (FP32 face work in difference variables, FP64 state,
+// primitives, ghosts, boundary fluxes and update).
+#include "kernels_mixed.cuh"
 #include "launch.hpp"
 
 namespace nf {
@@ -48,11 +50,24 @@ void launch_gradient_fast(const MeshView<double>& m, const StageArgs& a, Launch 
 void launch_flux_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
   NF_NODE_DISPATCH(flux_node_kernel, double, m, a, l);
 }
+// mixed form (difference variables, kernels_mixed.cuh)
+#define NF_DELTA_DISPATCH(KERNEL, m, a, l)                                                         \
+  do {                                                                                              \
+    const int b = fast_block(l.block);                                                             \
+    const int g = grid_for(m.n, b);                                                                \
+    switch (l.variant) {                                                                            \
+      case 1: KERNEL<true, 1><<<g, b, 0, l.stream>>>(m, a); break;                                 \
+      case 2: KERNEL<false, kCap<float>><<<g, b, 0, l.stream>>>(m, a); break;                      \
+      case 3: KERNEL<true, kCap<float>><<<g, b, 0, l.stream>>>(m, a); break;                       \
+      default: KERNEL<false, 1><<<g, b, 0, l.stream>>>(m, a); break;                               \
+    }                                                                                               \
+  } while (0)
+
 void launch_gradient_mixed(const MeshView<float>& m, const StageArgs& a, Launch l) {
-  NF_NODE_DISPATCH(gradient_node_kernel, float, m, a, l);
+  NF_DELTA_DISPATCH(gradient_delta_kernel, m, a, l);
 }
 void launch_flux_mixed(const MeshView<float>& m, const StageArgs& a, Launch l) {
-  NF_NODE_DISPATCH(flux_node_kernel, float, m, a, l);
+  NF_DELTA_DISPATCH(flux_delta_kernel, m, a, l);
 }
 void launch_ghost_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
   if (m.nb > 0) ghost_kernel<double, false><<<grid_for(m.nb, l.block), l.block, 0, l.stream>>>(m, a);
@@ -60,11 +75,8 @@ void launch_ghost_fast(const MeshView<double>& m, const StageArgs& a, Launch l) 
 void launch_bflux_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
   if (m.nb > 0) boundary_flux_kernel<double, false><<<grid_for(m.nb, l.block), l.block, 0, l.stream>>>(m, a);
 }
-void launch_ghost_mixed(const MeshView<float>& m, const StageArgs& a, Launch l) {
-  if (m.nb > 0) ghost_kernel<float, false><<<grid_for(m.nb, l.block), l.block, 0, l.stream>>>(m, a);
-}
-void launch_bflux_mixed(const MeshView<float>& m, const StageArgs& a, Launch l) {
-  if (m.nb > 0) boundary_flux_kernel<float, false><<<grid_for(m.nb, l.block), l.block, 0, l.stream>>>(m, a);
+void launch_bflux_mixed(const MeshView<double>& m, const StageArgs& a, Launch l) {
+  if (m.nb > 0) boundary_flux_delta_kernel<<<grid_for(m.nb, l.block), l.block, 0, l.stream>>>(m, a);
 }
 void launch_prim_fast(int n, int stride, const double* U, double* V, float* V32, Launch l) {
   prim_kernel_fast<false><<<grid_for(n, l.block), l.block, 0, l.stream>>>(n, stride, U, V, V32);

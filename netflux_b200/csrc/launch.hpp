@@ -30,8 +30,9 @@ void launch_gradient_mixed(const MeshView<float>& m, const StageArgs& a, Launch 
 void launch_flux_mixed(const MeshView<float>& m, const StageArgs& a, Launch l);
 void launch_ghost_fast(const MeshView<double>& m, const StageArgs& a, Launch l);
 void launch_bflux_fast(const MeshView<double>& m, const StageArgs& a, Launch l);
-void launch_ghost_mixed(const MeshView<float>& m, const StageArgs& a, Launch l);
-void launch_bflux_mixed(const MeshView<float>& m, const StageArgs& a, Launch l);
+// mixed: ghosts come from launch_ghost_fast (FP64); boundary fluxes are
+// stored as FP32 differences to the owner's physical flux
+void launch_bflux_mixed(const MeshView<double>& m, const StageArgs& a, Launch l);
 void launch_prim_fast(int n, int stride, const double* U, double* V, float* V32, Launch l);
 
 }  // namespace nf

@@ -164,12 +164,12 @@ struct nf_solver {
   DevBuf<int> slot, nbslot, b_cell, b_slot, b_face, b_patch, b_slotf;
   DevBuf<int> cnode, gcode, nbvf, nbsf;  // node-based layout of the fast forms
   DevBuf<double> S, nhat, area, rs, vol, dS, nodes4;
-  DevBuf<float> S32, nhat32, area32, rs32, nodes4_32;
+  DevBuf<float> nodes4_32;
   int nb = 0, bstride = 0;
   DevBuf<nf::PatchBC> patches;
   // state
   DevBuf<double> U, W, V0, V1, fs, grad, phi, R, dt_local, res_cell, scal, part, res_out, vg, fb;
-  DevBuf<float> V32a, V32b, fs32, grad32, phi32, vg32, fb32;
+  DevBuf<float> fs32, grad32, phi32, fb32;  // mixed: increments, fields, boundary flux differences
   DevBuf<unsigned> status;
   DevBuf<long long> chunk_begin, chunk_end, case_cells;
   DevBuf<int> case_chunk0;
@@ -222,7 +222,6 @@ struct nf_solver {
   }
 
   double* Vbuf(int i) { return i ? V1.p : V0.p; }
-  float* V32buf(int i) { return i ? V32b.p : V32a.p; }
   nf::Launch launch() const { return nf::Launch{block, stream}; }
 
   nf::MeshView<double> view64() const {
@@ -232,7 +231,7 @@ struct nf_solver {
                                 bstride, b_cell.p, b_slot.p, b_face.p, b_patch.p, fast ? b_slotf.p : b_slot.p};
   }
   nf::MeshView<float> view32() const {
-    return nf::MeshView<float>{n, stride, n_faces, slot.p, nbslot.p, S32.p, nhat32.p, area32.p, rs32.p,
+    return nf::MeshView<float>{n, stride, n_faces, slot.p, nbslot.p, nullptr, nullptr, nullptr, nullptr,
                                nodes4_32.p, cnode.p, gcode.p, nbvf.p, nbsf.p, vol.p, dS.p, patches.p, nb,
                                bstride, b_cell.p, b_slot.p, b_face.p, b_patch.p, b_slotf.p};
   }
@@ -347,18 +346,13 @@ struct nf_solver {
     a.fs = fs.p;
     a.vg = vg.p;
     a.fb = fb.p;
-    a.vg32 = vg32.p;
     a.fb32 = fb32.p;
     a.dt_local = dt_local.p;
     a.scal = scal.p;
     a.status = status.p;
     a.Uin = U.p;
     a.Uout = W.p;
-    if (p.precision == NF_PREC_MIXED) {
-      a.Vin32 = V32buf(vcur);
-      a.Vout32 = V32buf(1 - vcur);
-      a.fs32 = fs32.p;
-    }
+    a.fs32 = fs32.p;
     return a;
   }
 
@@ -371,13 +365,6 @@ struct nf_solver {
     std::vector<double> keep(size_t(5) * stride);
     ck(cudaMemcpyAsync(keep.data(), Vbuf(other), keep.size() * sizeof(double), cudaMemcpyDeviceToHost, stream),
        "tune save");
-    std::vector<float> keep32;
-    if (p.precision == NF_PREC_MIXED) {
-      keep32.resize(size_t(5) * stride);
-      ck(cudaMemcpyAsync(keep32.data(), V32buf(other), keep32.size() * sizeof(float), cudaMemcpyDeviceToHost,
-                         stream),
-         "tune save");
-    }
     ck(cudaStreamSynchronize(stream), "tune sync");
     nf::StageArgs a = first_stage_args();
     cudaEvent_t e0, e1;
@@ -395,8 +382,7 @@ struct nf_solver {
     };
     const KCfg cands[] = {{128, 0}, {128, 1}, {128, 2}, {128, 3}, {64, 0}, {64, 1}, {64, 2}, {64, 3}};
     if (a.second_order) {
-      if (p.precision == NF_PREC_MIXED) nf::launch_ghost_mixed(view32(), a, launch());
-      else nf::launch_ghost_fast(view64(), a, launch());
+      nf::launch_ghost_fast(view64(), a, launch());
       float best = 1e30f;
       for (const KCfg& k : cands) {
         const float t = time_it([&] { launch_gradient(a, k); });
@@ -407,7 +393,7 @@ struct nf_solver {
       }
       launch_gradient(a, kgrad);
     }
-    if (p.precision == NF_PREC_MIXED) nf::launch_bflux_mixed(view32(), a, launch());
+    if (p.precision == NF_PREC_MIXED) nf::launch_bflux_mixed(view64(), a, launch());
     else nf::launch_bflux_fast(view64(), a, launch());
     float best = 1e30f;
     for (const KCfg& k : cands) {
@@ -421,10 +407,6 @@ struct nf_solver {
     cudaEventDestroy(e1);
     ck(cudaMemcpyAsync(Vbuf(other), keep.data(), keep.size() * sizeof(double), cudaMemcpyHostToDevice, stream),
        "tune restore");
-    if (!keep32.empty())
-      ck(cudaMemcpyAsync(V32buf(other), keep32.data(), keep32.size() * sizeof(float), cudaMemcpyHostToDevice,
-                         stream),
-         "tune restore");
     ck(cudaMemsetAsync(status.p, 0, sizeof(unsigned), stream), "status reset");
     ck(cudaStreamSynchronize(stream), "tune sync");
     for (auto& g : graph)
@@ -449,7 +431,6 @@ struct nf_solver {
       a.fs = fs.p;
       a.vg = vg.p;
       a.fb = fb.p;
-      a.vg32 = vg32.p;
       a.fb32 = fb32.p;
       a.grad = p.keep_stage_fields ? grad.p : nullptr;
       a.phi = p.keep_stage_fields ? phi.p : nullptr;
@@ -480,24 +461,21 @@ struct nf_solver {
         a.Uout = U.p;
       }
       if (p.precision == NF_PREC_MIXED) {
-        a.Vin32 = V32buf(vcur);
-        a.Vout32 = V32buf(1 - vcur);
         a.fs32 = fs32.p;
         a.grad32 = p.keep_stage_fields ? grad32.p : nullptr;
         a.phi32 = p.keep_stage_fields ? phi32.p : nullptr;
       }
       if (a.second_order) {
         prof_begin(NF_KERNEL_OTHER);
-        if (p.precision == NF_PREC_MIXED) nf::launch_ghost_mixed(view32(), a, launch());
-        else if (p.precision == NF_PREC_FP64) nf::launch_ghost_fast(view64(), a, launch());
-        else nf::launch_ghost_ref(view64(), a, launch());
+        if (p.precision == NF_PREC_FP64_REF) nf::launch_ghost_ref(view64(), a, launch());
+        else nf::launch_ghost_fast(view64(), a, launch());
         prof_end();
         prof_begin(NF_KERNEL_GRADIENT);
         launch_gradient(a, kgrad);
         prof_end();
       }
       prof_begin(NF_KERNEL_OTHER);
-      if (p.precision == NF_PREC_MIXED) nf::launch_bflux_mixed(view32(), a, launch());
+      if (p.precision == NF_PREC_MIXED) nf::launch_bflux_mixed(view64(), a, launch());
       else if (p.precision == NF_PREC_FP64) nf::launch_bflux_fast(view64(), a, launch());
       else nf::launch_bflux_ref(view64(), a, launch());
       prof_end();
@@ -950,24 +928,9 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     s->dS.upload(h_dS, st);
     s->patches.upload(h_pb, st);
     if (p.precision == NF_PREC_MIXED) {
-      auto tof = [](const std::vector<double>& v) {
-        std::vector<float> o(v.size());
-        for (size_t i = 0; i < v.size(); i++) o[i] = float(v[i]);
-        return o;
-      };
-      s->S32.upload(tof(h_S), st);
-      s->nhat32.upload(tof(h_n), st);
-      s->area32.upload(tof(h_a), st);
-      s->rs32.upload(tof(h_rs), st);
-      s->vg32.alloc(size_t(5) * s->bstride);
       s->fb32.alloc(size_t(5) * s->bstride);
-      s->vg32.zero(st);
       s->fb32.zero(st);
-      s->V32a.alloc(size_t(5) * stride);
-      s->V32b.alloc(size_t(5) * stride);
       s->fs32.alloc(size_t(20) * stride);
-      s->V32a.zero(st);
-      s->V32b.zero(st);
       s->fs32.zero(st);
       if (p.keep_stage_fields) {
         s->grad32.alloc(size_t(15) * stride);
@@ -980,12 +943,12 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     s->W.alloc(size_t(5) * stride);
     s->V0.alloc(size_t(5) * stride);
     s->V1.alloc(size_t(5) * stride);
+    s->vg.alloc(size_t(5) * s->bstride);  // FP64 ghosts in every form
+    s->vg.zero(st);
     if (p.precision != NF_PREC_MIXED) {
       s->fs.alloc(size_t(20) * stride);
       s->fs.zero(st);
-      s->vg.alloc(size_t(5) * s->bstride);
       s->fb.alloc(size_t(5) * s->bstride);
-      s->vg.zero(st);
       s->fb.zero(st);
     }
     if (p.keep_stage_fields) {
@@ -1079,9 +1042,8 @@ int nf_set_state(nf_solver* s, const double* U, int64_t n_cells) {
     // primitives of the initial state in both buffers (the first
     // calc_timestep reads them, like the harness-initialised reference)
     for (int b = 0; b < 2; b++) {
-      float* v32 = s->p.precision == NF_PREC_MIXED ? s->V32buf(b) : nullptr;
-      if (s->p.precision == NF_PREC_FP64_REF) nf::launch_prim_ref(s->n, st, s->U.p, s->Vbuf(b), v32, s->launch());
-      else nf::launch_prim_fast(s->n, st, s->U.p, s->Vbuf(b), v32, s->launch());
+      if (s->p.precision == NF_PREC_FP64_REF) nf::launch_prim_ref(s->n, st, s->U.p, s->Vbuf(b), nullptr, s->launch());
+      else nf::launch_prim_fast(s->n, st, s->U.p, s->Vbuf(b), nullptr, s->launch());
     }
     s->vcur = 0;
     s->stepped = false;
