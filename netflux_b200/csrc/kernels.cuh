@@ -86,16 +86,14 @@ struct StageArgs {
   const double* dt_local;
   const double* scal;    // device scalars: [0] dt (min target), [1] time, [2] t_end
   unsigned* status;
-  // mixed precision: FP32 copies of the primitives, face states and fields
-  const float* Vin32;
-  float* Vout32;
+  // mixed form: FP32 reconstruction increments and fields
   float* fs32;
   float* grad32;
   float* phi32;
-  // boundary faces: cell-centre ghost states [5][bstride] and boundary fluxes [5][bstride]
+  // boundary faces: cell-centre ghost states [5][bstride] and boundary fluxes
+  // [5][bstride] (mixed form: FP32 differences to the owner's physical flux)
   double* vg;
   double* fb;
-  float* vg32;
   float* fb32;
   // limiter ratchet (extension): per-cell case, per-case switch (null: off)
   // and the kept limiter values [5][stride] (FP64 or FP32 with the state form)
@@ -133,10 +131,12 @@ __device__ __forceinline__ double stage_dt(const double* scal) {
   return dt;
 }
 
+// The templated kernels below run in FP64 (T = double); the mixed form has
+// its own kernels (kernels_mixed.cuh).
 template <typename T>
 __device__ __forceinline__ T ld_v(const StageArgs& a, int idx) {
-  if constexpr (sizeof(T) == 8) return a.Vin[idx];
-  else return a.Vin32[idx];
+  static_assert(sizeof(T) == 8, "FP64 kernels");
+  return a.Vin[idx];
 }
 
 // Four threads per cell: lane q of a quad owns the cell's face slot q. A
@@ -219,8 +219,7 @@ __global__ void __launch_bounds__(256) gradient_limiter_kernel(MeshView<T> m, St
     const bool own = (sl[q] & 1) == 0;
     T vo;
     if (ns[q] >= 0) vo = ld_v<T>(a, k * st + (ns[q] >> 2));
-    else if constexpr (sizeof(T) == 8) vo = a.vg[k * m.bstride + (-ns[q] - 1)];
-    else vo = a.vg32[k * m.bstride + (-ns[q] - 1)];
+    else vo = a.vg[k * m.bstride + (-ns[q] - 1)];
     // the neighbour side subtracts its term: (-x)/v == -(x/v) and
     // g + (-y) == g - y exactly, so a signed normal reproduces both branches
     const T s0 = m.S[f], s1 = m.S[F + f], s2 = m.S[2 * F + f];
@@ -277,22 +276,12 @@ __global__ void __launch_bounds__(256) gradient_limiter_kernel(MeshView<T> m, St
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     if (sl[q] < 0) continue;
-    const T v = vc + phi * gr[q];
-    if constexpr (sizeof(T) == 8) a.fs[(q * 5 + k) * st + c] = v;
-    else a.fs32[(q * 5 + k) * st + c] = v;
+    a.fs[(q * 5 + k) * st + c] = vc + phi * gr[q];
   }
-  if constexpr (sizeof(T) == 8) {
-    if (a.grad) {
+  if (a.grad) {
 #pragma unroll
-      for (int d = 0; d < 3; d++) a.grad[(k * 3 + d) * st + c] = g[d];
-      a.phi[k * st + c] = phi;
-    }
-  } else {
-    if (a.grad32) {
-#pragma unroll
-      for (int d = 0; d < 3; d++) a.grad32[(k * 3 + d) * st + c] = g[d];
-      a.phi32[k * st + c] = phi;
-    }
+    for (int d = 0; d < 3; d++) a.grad[(k * 3 + d) * st + c] = g[d];
+    a.phi[k * st + c] = phi;
   }
 }
 
@@ -323,10 +312,7 @@ __global__ void __launch_bounds__(256) flux_update_kernel(MeshView<T> m, StageAr
     // boundary face (this cell is its owner): flux from boundary_flux_kernel
     const int b = -ns - 1;
 #pragma unroll
-    for (int k = 0; k < 5; k++) {
-      if constexpr (sizeof(T) == 8) contrib[k] = -a.fb[k * m.bstride + b];
-      else contrib[k] = -double(a.fb32[k * m.bstride + b]);
-    }
+    for (int k = 0; k < 5; k++) contrib[k] = -a.fb[k * m.bstride + b];
   } else if (has) {
     const int f = sl >> 1;
     const T nh[3] = {m.nhat[f], m.nhat[F + f], m.nhat[2 * F + f]};
@@ -336,13 +322,8 @@ __global__ void __launch_bounds__(256) flux_update_kernel(MeshView<T> m, StageAr
 #pragma unroll
     for (int k = 0; k < 5; k++) {
       if (second) {
-        if constexpr (sizeof(T) == 8) {
-          Vs[k] = a.fs[(q * 5 + k) * st + c];
-          Vx[k] = a.fs[(q2 * 5 + k) * st + o];
-        } else {
-          Vs[k] = a.fs32[(q * 5 + k) * st + c];
-          Vx[k] = a.fs32[(q2 * 5 + k) * st + o];
-        }
+        Vs[k] = a.fs[(q * 5 + k) * st + c];
+        Vx[k] = a.fs[(q2 * 5 + k) * st + o];
       } else {
         Vs[k] = ld_v<T>(a, k * st + c);
         Vx[k] = ld_v<T>(a, k * st + o);
@@ -406,8 +387,7 @@ __global__ void __launch_bounds__(256) flux_update_kernel(MeshView<T> m, StageAr
     if (k == q || (k == 4 && q == 0)) {
       a.Uout[k * st + c] = Unew[k];
       a.Vout[k * st + c] = Vn[k];
-      if (a.Vout32) a.Vout32[k * st + c] = float(Vn[k]);
-      if (a.R) a.R[k * st + c] = R[k];
+        if (a.R) a.R[k * st + c] = R[k];
     }
   }
   if (q == 0) {
@@ -478,18 +458,10 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.n) return;
   const int st = m.stride;
-  const T* Vin = nullptr;
-  const T* Vg = nullptr;
-  T* fs = nullptr;
-  if constexpr (sizeof(T) == 8) {
-    Vin = reinterpret_cast<const T*>(a.Vin);
-    Vg = reinterpret_cast<const T*>(a.vg);
-    fs = reinterpret_cast<T*>(a.fs);
-  } else {
-    Vin = reinterpret_cast<const T*>(a.Vin32);
-    Vg = reinterpret_cast<const T*>(a.vg32);
-    fs = reinterpret_cast<T*>(a.fs32);
-  }
+  static_assert(sizeof(T) == 8, "FP64 kernel");
+  const T* Vin = a.Vin;
+  const T* Vg = a.vg;
+  T* fs = a.fs;
   int nb[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) nb[q] = m.nbvf[q * st + c];
@@ -566,18 +538,10 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
     }
 #pragma unroll
     for (int q = 0; q < 4; q++) fs[(q * 5 + k) * st + c] = fma(phi, gr[q], vc);
-    if constexpr (sizeof(T) == 8) {
-      if (a.grad) {
+    if (a.grad) {
 #pragma unroll
-        for (int e = 0; e < 3; e++) a.grad[(k * 3 + e) * st + c] = g[e];
-        a.phi[k * st + c] = phi;
-      }
-    } else {
-      if (a.grad32) {
-#pragma unroll
-        for (int e = 0; e < 3; e++) a.grad32[(k * 3 + e) * st + c] = g[e];
-        a.phi32[k * st + c] = phi;
-      }
+      for (int e = 0; e < 3; e++) a.grad[(k * 3 + e) * st + c] = g[e];
+      a.phi[k * st + c] = phi;
     }
   }
 }
@@ -624,7 +588,6 @@ __device__ __forceinline__ void stage_update(const StageArgs& a, int c, int st, 
   for (int k = 0; k < 5; k++) {
     a.Uout[k * st + c] = Unew[k];
     a.Vout[k * st + c] = Vn[k];
-    if (a.Vout32) a.Vout32[k * st + c] = float(Vn[k]);
     if (a.R) a.R[k * st + c] = R[k];
     finite = finite && isfinite(R[k]) && isfinite(Unew[k]);
   }
@@ -639,18 +602,10 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
   if (c >= m.n) return;
   const int st = m.stride;
   const bool second = a.second_order != 0;
-  const T* fsb = nullptr;
-  const T* Vin = nullptr;
-  const T* fb = nullptr;
-  if constexpr (sizeof(T) == 8) {
-    fsb = reinterpret_cast<const T*>(a.fs);
-    Vin = reinterpret_cast<const T*>(a.Vin);
-    fb = reinterpret_cast<const T*>(a.fb);
-  } else {
-    fsb = reinterpret_cast<const T*>(a.fs32);
-    Vin = reinterpret_cast<const T*>(a.Vin32);
-    fb = reinterpret_cast<const T*>(a.fb32);
-  }
+  static_assert(sizeof(T) == 8, "FP64 kernel");
+  const T* fsb = a.fs;
+  const T* Vin = a.Vin;
+  const T* fb = a.fb;
   const int code = m.gcode[c];
   int ns[4];
 #pragma unroll
@@ -737,8 +692,7 @@ __global__ void __launch_bounds__(256) ghost_kernel(MeshView<T> m, StageArgs a) 
   ghost_state<T>(m.patches[m.b_patch[b]], V, nh, G);
 #pragma unroll
   for (int k = 0; k < 5; k++) {
-    if constexpr (sizeof(T) == 8) a.vg[k * m.bstride + b] = G[k];
-    else a.vg32[k * m.bstride + b] = G[k];
+    a.vg[k * m.bstride + b] = G[k];
   }
 }
 
@@ -752,8 +706,7 @@ __global__ void __launch_bounds__(256) boundary_flux_kernel(MeshView<T> m, Stage
 #pragma unroll
   for (int k = 0; k < 5; k++) {
     if (a.second_order) {
-      if constexpr (sizeof(T) == 8) VL[k] = a.fs[(q * 5 + k) * st + c];
-      else VL[k] = a.fs32[(q * 5 + k) * st + c];
+      VL[k] = a.fs[(q * 5 + k) * st + c];
     } else {
       VL[k] = ld_v<T>(a, k * st + c);
     }
@@ -770,10 +723,7 @@ __global__ void __launch_bounds__(256) boundary_flux_kernel(MeshView<T> m, Stage
     rusanov_fast<T>(VL, VR, nh, m.area[f], Fl);
   }
 #pragma unroll
-  for (int k = 0; k < 5; k++) {
-    if constexpr (sizeof(T) == 8) a.fb[k * m.bstride + b] = Fl[k];
-    else a.fb32[k * m.bstride + b] = Fl[k];
-  }
+  for (int k = 0; k < 5; k++) a.fb[k * m.bstride + b] = Fl[k];
 }
 
 // ---------------------------------------------------------------------------
