@@ -202,6 +202,13 @@ int nf_advance(nf_solver* s, int64_t n_steps, double* time_out);
  * Driver.cpp:31-57). */
 int nf_solve_steady(nf_solver* s, double tol, int64_t max_steps, int check_every, int64_t* steps_per_case,
                     double* res0_per_case, double* res_per_case, double* ms_per_case);
+/* The same with an absolute density-residual target per case
+ * (res_target[n_cases]), e.g. the tolerance times the residual of a
+ * free-stream start, so that a warm-started solve stops at the same residual
+ * as the plain one. A case already at its target after the first step stops
+ * there. */
+int nf_solve_steady_to(nf_solver* s, const double* res_target, int64_t max_steps, int check_every,
+                       int64_t* steps_per_case, double* res0_per_case, double* res_per_case, double* ms_per_case);
 
 /* Density residual of the first stage of the last step: RMS and max of
  * R_rho,i / vol_i over all cells (per case: n_cases pairs). */
@@ -250,6 +257,40 @@ void nf_destroy(nf_solver* s);
  * the array and race. It has no counterpart in the reference, which computes
  * no residual norms. */
 int nf_residual_norms_noalloc(const double* values, int64_t n, double* out, void* stream);
+
+
+/* ------------------------------------------------------------------------
+ * Surrogate MLP for warm starts (extension; the reference has no learned
+ * part). 7 inputs (cell centroid x, y, z, wall distance, Mach, bump height,
+ * each normalised by the caller) -> 4 hidden layers of 128 SiLU units -> 5
+ * outputs (the caller's normalised conserved variables). BF16 weights and
+ * activations with FP32 accumulation on the tensor cores; FP32 master weights
+ * and Adam (beta 0.9/0.999, eps 1e-8). Parameters (FP32, nf_mlp_param_count
+ * values, padded shapes): W0 [128][16] (columns 0..6 inputs, column 7 bias),
+ * W1, W2, W3 [128][128], b1, b2, b3 [128], W4 [16][128] (rows 0..4), b4 [16].
+ * ------------------------------------------------------------------------ */
+typedef struct nf_mlp nf_mlp;
+int nf_mlp_param_count(void);
+nf_mlp* nf_mlp_create(uint64_t seed);
+const char* nf_mlp_last_error(const nf_mlp* m);
+void nf_mlp_destroy(nf_mlp* m);
+int nf_mlp_get_params(nf_mlp* m, float* out);
+int nf_mlp_set_params(nf_mlp* m, const float* in);
+/* Training set: features [n][7], targets [n][5] (copied to the device). */
+int nf_mlp_set_data(nf_mlp* m, const float* features, const float* targets, int64_t n);
+/* steps of Adam on uniformly drawn batches of `batch` samples (mean squared
+ * error over the 5 outputs); loss_report[n_report]: the loss of the last step
+ * of each of n_report equal segments; *ms_out the device time. */
+int nf_mlp_train(nf_mlp* m, int64_t steps, int64_t batch, float lr, uint64_t seed, int n_report,
+                 double* loss_report, double* ms_out);
+/* Gradient of the mean squared error over the given samples (no update). */
+int nf_mlp_gradients(nf_mlp* m, const float* features, const float* targets, int64_t n, float* grad_out,
+                     double* loss_out);
+/* Forward pass: out [n][5]; *ms_out the device time of the kernel. */
+int nf_mlp_predict(nf_mlp* m, const float* features, int64_t n, float* out, double* ms_out);
+/* D[128][N] = A[128][K] B[N][K]^T through the library's tcgen05 path
+ * (A, B as BF16 bit patterns, row-major); 16 <= N, K <= 256, multiples of 16. */
+int nf_mlp_gemm_selftest(const uint16_t* A, const uint16_t* B, int N, int K, float* D);
 
 #ifdef __cplusplus
 }

@@ -30,7 +30,10 @@ EXPORTED = (
     "nf_mesh_export", "nf_mesh_get_permutation", "nf_mesh_get_case_offsets", "nf_mesh_destroy",
     "nf_params_default", "nf_create", "nf_set_state", "nf_get_state", "nf_calc_timestep", "nf_set_timestep",
     "nf_step", "nf_advance", "nf_get_residual", "nf_get_field", "nf_synchronize", "nf_last_error", "nf_destroy",
-    "nf_time_steps", "nf_residual_norms_noalloc", "nf_tune", "nf_solve_steady",
+    "nf_time_steps", "nf_residual_norms_noalloc", "nf_tune", "nf_solve_steady", "nf_solve_steady_to",
+    "nf_mlp_param_count", "nf_mlp_create", "nf_mlp_last_error", "nf_mlp_destroy", "nf_mlp_get_params",
+    "nf_mlp_set_params", "nf_mlp_set_data", "nf_mlp_train", "nf_mlp_gradients", "nf_mlp_predict",
+    "nf_mlp_gemm_selftest",
 )
 NF_KERNEL_TIMESTEP, NF_KERNEL_GRADIENT, NF_KERNEL_FLUX, NF_KERNEL_OTHER, NF_KERNEL_COUNT = range(5)
 
@@ -75,6 +78,7 @@ def load() -> C.CDLL:
     lib = C.CDLL(LIB_PATH)
     P, I64, I, D = C.c_void_p, C.c_int64, C.c_int, C.c_double
     dp, i64p, u32p = C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_uint32)
+    fp = C.POINTER(C.c_float)
     sig = {
         "nf_mesh_from_su2": (P, [C.c_char_p, I, C.POINTER(C.c_char_p), C.POINTER(C.c_int)]),
         "nf_mesh_from_arrays": (P, [I64, dp, I64, i64p, I, C.POINTER(C.c_char_p), C.POINTER(C.c_int), i64p, i64p]),
@@ -102,6 +106,19 @@ def load() -> C.CDLL:
         "nf_residual_norms_noalloc": (I, [P, I64, P, P]),
         "nf_tune": (I, [P, C.POINTER(C.c_int)]),
         "nf_solve_steady": (I, [P, D, I64, I, i64p, dp, dp, dp]),
+        "nf_solve_steady_to": (I, [P, dp, I64, I, i64p, dp, dp, dp]),
+        # surrogate MLP
+        "nf_mlp_param_count": (I, []),
+        "nf_mlp_create": (P, [C.c_uint64]),
+        "nf_mlp_last_error": (C.c_char_p, [P]),
+        "nf_mlp_destroy": (None, [P]),
+        "nf_mlp_get_params": (I, [P, fp]),
+        "nf_mlp_set_params": (I, [P, fp]),
+        "nf_mlp_set_data": (I, [P, fp, fp, I64]),
+        "nf_mlp_train": (I, [P, I64, I64, C.c_float, C.c_uint64, I, dp, dp]),
+        "nf_mlp_gradients": (I, [P, fp, fp, I64, fp, dp]),
+        "nf_mlp_predict": (I, [P, fp, I64, fp, dp]),
+        "nf_mlp_gemm_selftest": (I, [C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), I, I, fp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -117,6 +134,10 @@ def dptr(a: np.ndarray):
 
 def i64ptr(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+def fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
 def u32ptr(a: np.ndarray):

@@ -1,0 +1,1009 @@
+// Surrogate MLP for warm starts (extension; the reference has no learned
+// part): 7 inputs (cell centroid, wall distance, Mach, bump height) ->
+// 4 hidden layers of 128 SiLU units -> 5 outputs (conserved variables
+// normalised by the free stream). BF16 weights and activations, FP32
+// accumulation in tensor memory, hand-written tcgen05 kernels:
+//   mlp_forward_kernel     all five layers of a 128-sample tile in one CTA,
+//                          weights resident in shared memory, the TMEM
+//                          accumulator turned into the next layer's operand by
+//                          the SiLU epilogue; optionally saves activations and
+//                          the loss gradient
+//   mlp_backward_kernel    the same structure backwards (transposed weights,
+//                          SiLU derivative in the epilogue) -> dZ of each layer
+//   mlp_wgrad_kernel       dW = dZ^T H over the batch (split over CTAs), batch
+//                          tiles transposed while staged, five accumulators in
+//                          TMEM, bias gradients through a column of ones
+//   mlp_adam_kernel        sums the per-CTA partial gradients, Adam update of
+//                          the FP32 master weights, BF16 operand images
+// Parameters in FP32 (padded shapes): W0 [128][16] (inputs 0..6, bias in
+// column 7), W1..W3 [128][128], b1..b3 [128], W4 [16][128] (rows 0..4 used),
+// b4 [16].
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/netflux_b200.h"
+#include "umma.cuh"
+
+namespace nf {
+namespace mlp {
+
+constexpr int H = 128;    // hidden width
+constexpr int KIN = 16;   // 7 inputs, a constant 1 (bias) and padding
+constexpr int NOUT = 16;  // 5 outputs and padding
+constexpr int NIN = 7;
+constexpr int NO = 5;
+constexpr int TILE = 128;  // samples per tile (MMA M)
+constexpr int KC = 64;     // batch rows per weight-gradient chunk
+constexpr int NAUG = H + 16;  // H columns, a column of ones, padding
+constexpr long long kWaitCycles = 4000000000LL;  // about 2 s
+
+constexpr int OFF_W0 = 0;
+constexpr int OFF_W1 = OFF_W0 + H * KIN;
+constexpr int OFF_W2 = OFF_W1 + H * H;
+constexpr int OFF_W3 = OFF_W2 + H * H;
+constexpr int OFF_B1 = OFF_W3 + H * H;
+constexpr int OFF_B2 = OFF_B1 + H;
+constexpr int OFF_B3 = OFF_B2 + H;
+constexpr int OFF_W4 = OFF_B3 + H;
+constexpr int OFF_B4 = OFF_W4 + NOUT * H;
+constexpr int N_PARAM = OFF_B4 + NOUT;
+
+// BF16 operand images, byte offsets; each is a K-major tile as it sits in
+// shared memory. Forward: W_l as [out][in]; backward: W_l^T as [in][out].
+constexpr int IMG_W0 = 0;
+constexpr int IMG_W1 = IMG_W0 + H * KIN * 2;
+constexpr int IMG_W2 = IMG_W1 + H * H * 2;
+constexpr int IMG_W3 = IMG_W2 + H * H * 2;
+constexpr int IMG_W4 = IMG_W3 + H * H * 2;
+constexpr int IMG_FWD = IMG_W4 + NOUT * H * 2;
+constexpr int IMG_T1 = 0;
+constexpr int IMG_T2 = IMG_T1 + H * H * 2;
+constexpr int IMG_T3 = IMG_T2 + H * H * 2;
+constexpr int IMG_T4 = IMG_T3 + H * H * 2;
+constexpr int IMG_BWD = IMG_T4 + H * NOUT * 2;
+
+// saved activations, element offsets in units of BF16 for B samples
+__host__ __device__ inline int64_t save_x0(int64_t) { return 0; }
+__host__ __device__ inline int64_t save_z(int64_t B, int l) { return B * KIN + (2 * l) * B * H; }
+__host__ __device__ inline int64_t save_h(int64_t B, int l) { return B * KIN + (2 * l + 1) * B * H; }
+__host__ __device__ inline int64_t save_size(int64_t B) { return B * KIN + 8 * B * H; }
+
+__device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
+__device__ __forceinline__ float dsilu(float z) {
+  const float s = 1.0f / (1.0f + expf(-z));
+  return s * (1.0f + z * (1.0f - s));
+}
+
+// pack 8 floats to 8 BF16 (round to nearest even) in a 16-byte vector
+__device__ __forceinline__ uint4 pack8(const float* v) {
+  uint4 r;
+  uint32_t* w = reinterpret_cast<uint32_t*>(&r);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const __nv_bfloat162 p = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    w[i] = *reinterpret_cast<const uint32_t*>(&p);
+  }
+  return r;
+}
+__device__ __forceinline__ void unpack8(uint4 r, float* v) {
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(&r);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const __nv_bfloat162 p = *reinterpret_cast<const __nv_bfloat162*>(&w[i]);
+    const float2 f = __bfloat1622float2(p);
+    v[2 * i] = f.x;
+    v[2 * i + 1] = f.y;
+  }
+}
+
+struct TileSync {
+  uint32_t mbar;
+  uint32_t phase = 0;
+  unsigned* status;
+  // wait for the MMAs committed to mbar; every thread agrees on the outcome
+  __device__ bool wait() {
+    const bool ok = umma::mbar_wait(mbar, phase, kWaitCycles);
+    phase ^= 1u;
+    const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    if (!all_ok && threadIdx.x == 0) atomicOr(status, 1u);
+    umma::fence_after_sync();
+    return all_ok;
+  }
+};
+
+// Common prologue: mbarrier, TMEM columns; returns the TMEM base address.
+__device__ uint32_t setup(uint64_t* mbar, uint32_t* tslot, uint32_t ncols) {
+  if (threadIdx.x == 0) {
+    umma::mbar_init(umma::smem_addr(mbar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (threadIdx.x < 32) umma::tmem_alloc(umma::smem_addr(tslot), ncols);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  return *tslot;
+}
+__device__ void teardown(uint32_t tbase, uint32_t ncols) {
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  if (threadIdx.x < 32) umma::tmem_dealloc(tbase, ncols);
+}
+
+// ---------------------------------------------------------------------------
+// Forward
+// ---------------------------------------------------------------------------
+struct FwdArgs {
+  const uint8_t* img;     // forward BF16 image
+  const float* params;    // FP32 master (biases b1..b4)
+  const float* feat;      // [n_all][7] normalised inputs
+  const float* target;    // [n_all][5] or null
+  const int64_t* idx;     // [B] sample of each row, or null (row b is sample b)
+  int64_t B;
+  float* out;             // [B][5] or null
+  __nv_bfloat16* save;    // saved activations (save_size(B)) or null
+  __nv_bfloat16* dz4;     // [B][16] loss gradient or null
+  double* loss;           // sum of squared errors (with target)
+  float loss_scale;       // d loss / d y = loss_scale * (y - t)
+  unsigned* status;
+};
+
+constexpr int FWD_SMEM = IMG_FWD + TILE * H * 2 + TILE * KIN * 2 + (3 * H + NOUT) * 4 + 64;
+
+__global__ void __launch_bounds__(128, 1) mlp_forward_kernel(FwdArgs a) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  uint8_t* s_img = sm;
+  uint8_t* s_act = sm + IMG_FWD;                 // [128 x K128] activations
+  uint8_t* s_x0 = s_act + TILE * H * 2;          // [128 x K16] inputs
+  float* s_bias = reinterpret_cast<float*>(s_x0 + TILE * KIN * 2);  // b1, b2, b3, b4
+  uint64_t* s_mbar = reinterpret_cast<uint64_t*>(s_bias + 3 * H + NOUT);
+  uint32_t* s_tslot = reinterpret_cast<uint32_t*>(s_mbar + 1);
+  const int t = threadIdx.x, w = t >> 5;
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(a.img);
+    uint4* dst = reinterpret_cast<uint4*>(s_img);
+    for (int i = t; i < IMG_FWD / 16; i += blockDim.x) dst[i] = src[i];
+    for (int i = t; i < 3 * H + NOUT; i += blockDim.x)
+      s_bias[i] = i < 3 * H ? a.params[OFF_B1 + i] : a.params[OFF_B4 + i - 3 * H];
+  }
+  const uint32_t tbase = setup(s_mbar, s_tslot, 128);
+  TileSync sync{umma::smem_addr(s_mbar), 0u, a.status};
+  const uint32_t lane_addr = tbase + (uint32_t(w * 32) << 16);
+  const uint32_t a_act = umma::smem_addr(s_act), a_x0 = umma::smem_addr(s_x0), a_img = umma::smem_addr(s_img);
+  const uint32_t id128 = umma::idesc_bf16(128, 128), id16 = umma::idesc_bf16(128, 16);
+  const int64_t n_tiles = (a.B + TILE - 1) / TILE;
+  float ssq = 0.f;
+  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int64_t b = tile * TILE + t;
+    const bool valid = b < a.B;
+    {  // inputs: 7 features, a constant 1 (bias of layer 0), zeros
+      float x[KIN];
+#pragma unroll
+      for (int k = 0; k < KIN; k++) x[k] = 0.f;
+      if (valid) {
+        const int64_t s = a.idx ? a.idx[b] : b;
+#pragma unroll
+        for (int k = 0; k < NIN; k++) x[k] = a.feat[s * NIN + k];
+        x[NIN] = 1.f;
+      }
+      const uint4 c0 = pack8(x), c1 = pack8(x + 8);
+      *reinterpret_cast<uint4*>(s_x0 + umma::kmaj_off(t, 0, KIN)) = c0;
+      *reinterpret_cast<uint4*>(s_x0 + umma::kmaj_off(t, 8, KIN)) = c1;
+      if (a.save && valid) {
+        uint4* g = reinterpret_cast<uint4*>(a.save + save_x0(a.B) + b * KIN);
+        g[0] = c0;
+        g[1] = c1;
+      }
+    }
+    umma::fence_async_shared();
+    __syncthreads();
+    for (int l = 0; l < 5; l++) {
+      if (t == 0) {
+        umma::fence_after_sync();
+        if (l == 0) {
+          umma::mma_bf16(tbase, umma::kmaj_desc(a_x0, KIN, 0), umma::kmaj_desc(a_img + IMG_W0, KIN, 0), id128, 0);
+        } else {
+          const int img = l == 1 ? IMG_W1 : l == 2 ? IMG_W2 : l == 3 ? IMG_W3 : IMG_W4;
+#pragma unroll 1
+          for (int s = 0; s < H / 16; s++)
+            umma::mma_bf16(tbase, umma::kmaj_desc(a_act, H, s), umma::kmaj_desc(a_img + img, H, s),
+                           l == 4 ? id16 : id128, s > 0 ? 1u : 0u);
+        }
+        umma::commit(sync.mbar);
+      }
+      if (!sync.wait()) goto done;
+      if (l < 4) {
+        // z = acc (+ bias), h = silu(z): the next layer's operand
+#pragma unroll 1
+        for (int c0 = 0; c0 < H; c0 += 32) {
+          float v[32];
+          umma::tmem_ld32(lane_addr + uint32_t(c0), v);
+          float z[32], h[32];
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            z[j] = l == 0 ? v[j] : v[j] + s_bias[(l - 1) * H + c0 + j];
+            h[j] = silu(z[j]);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const uint4 hv = pack8(h + 8 * q);
+            *reinterpret_cast<uint4*>(s_act + umma::kmaj_off(t, c0 + 8 * q, H)) = hv;
+            if (a.save && valid) {
+              *reinterpret_cast<uint4*>(a.save + save_z(a.B, l) + b * H + c0 + 8 * q) = pack8(z + 8 * q);
+              *reinterpret_cast<uint4*>(a.save + save_h(a.B, l) + b * H + c0 + 8 * q) = hv;
+            }
+          }
+        }
+      } else {
+        float v[16];
+        umma::tmem_ld16(lane_addr, v);
+        float y[NO];
+#pragma unroll
+        for (int o = 0; o < NO; o++) y[o] = v[o] + s_bias[3 * H + o];
+        if (valid) {
+          if (a.out)
+#pragma unroll
+            for (int o = 0; o < NO; o++) a.out[b * NO + o] = y[o];
+          if (a.target) {
+            const int64_t s = a.idx ? a.idx[b] : b;
+            float g[16];
+#pragma unroll
+            for (int o = 0; o < 16; o++) g[o] = 0.f;
+#pragma unroll
+            for (int o = 0; o < NO; o++) {
+              const float e = y[o] - a.target[s * NO + o];
+              ssq += e * e;
+              g[o] = a.loss_scale * e;
+            }
+            if (a.dz4) {
+              uint4* gd = reinterpret_cast<uint4*>(a.dz4 + b * NOUT);
+              gd[0] = pack8(g);
+              gd[1] = pack8(g + 8);
+            }
+          }
+        }
+      }
+      // TMEM read and operand written before the next MMA
+      umma::fence_before_sync();
+      umma::fence_async_shared();
+      __syncthreads();
+    }
+  }
+done:
+  if (a.loss) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) ssq += __shfl_xor_sync(0xffffffffu, ssq, off);
+    if ((t & 31) == 0 && ssq != 0.f) atomicAdd(a.loss, double(ssq));
+  }
+  teardown(tbase, 128);
+}
+
+// ---------------------------------------------------------------------------
+// Backward through the activations: dZ3, dZ2, dZ1, dZ0
+// ---------------------------------------------------------------------------
+struct BwdArgs {
+  const uint8_t* img;          // backward BF16 image (transposed weights)
+  const __nv_bfloat16* save;   // saved activations
+  const __nv_bfloat16* dz4;    // [B][16]
+  int64_t B;
+  __nv_bfloat16* dz;           // [4][B][128]: dZ0..dZ3
+  unsigned* status;
+};
+
+constexpr int BWD_SMEM = IMG_BWD + TILE * H * 2 + TILE * NOUT * 2 + 64;
+
+__global__ void __launch_bounds__(128, 1) mlp_backward_kernel(BwdArgs a) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  uint8_t* s_img = sm;
+  uint8_t* s_act = sm + IMG_BWD;
+  uint8_t* s_d4 = s_act + TILE * H * 2;
+  uint64_t* s_mbar = reinterpret_cast<uint64_t*>(s_d4 + TILE * NOUT * 2);
+  uint32_t* s_tslot = reinterpret_cast<uint32_t*>(s_mbar + 1);
+  const int t = threadIdx.x, w = t >> 5;
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(a.img);
+    uint4* dst = reinterpret_cast<uint4*>(s_img);
+    for (int i = t; i < IMG_BWD / 16; i += blockDim.x) dst[i] = src[i];
+  }
+  const uint32_t tbase = setup(s_mbar, s_tslot, 128);
+  TileSync sync{umma::smem_addr(s_mbar), 0u, a.status};
+  const uint32_t lane_addr = tbase + (uint32_t(w * 32) << 16);
+  const uint32_t a_act = umma::smem_addr(s_act), a_d4 = umma::smem_addr(s_d4), a_img = umma::smem_addr(s_img);
+  const uint32_t id128 = umma::idesc_bf16(128, 128);
+  const int64_t n_tiles = (a.B + TILE - 1) / TILE;
+  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int64_t b = tile * TILE + t;
+    const bool valid = b < a.B;
+    {
+      uint4 c0 = make_uint4(0, 0, 0, 0), c1 = c0;
+      if (valid) {
+        const uint4* g = reinterpret_cast<const uint4*>(a.dz4 + b * NOUT);
+        c0 = g[0];
+        c1 = g[1];
+      }
+      *reinterpret_cast<uint4*>(s_d4 + umma::kmaj_off(t, 0, NOUT)) = c0;
+      *reinterpret_cast<uint4*>(s_d4 + umma::kmaj_off(t, 8, NOUT)) = c1;
+    }
+    umma::fence_async_shared();
+    __syncthreads();
+    // layer l's input gradient: dH_{l-1} = dZ_l W_l, then dZ_{l-1} = dH_{l-1} silu'(Z_{l-1})
+    for (int l = 4; l >= 1; l--) {
+      if (t == 0) {
+        umma::fence_after_sync();
+        if (l == 4) {
+          umma::mma_bf16(tbase, umma::kmaj_desc(a_d4, NOUT, 0), umma::kmaj_desc(a_img + IMG_T4, NOUT, 0), id128, 0);
+        } else {
+          const int img = l == 1 ? IMG_T1 : l == 2 ? IMG_T2 : IMG_T3;
+#pragma unroll 1
+          for (int s = 0; s < H / 16; s++)
+            umma::mma_bf16(tbase, umma::kmaj_desc(a_act, H, s), umma::kmaj_desc(a_img + img, H, s), id128,
+                           s > 0 ? 1u : 0u);
+        }
+        umma::commit(sync.mbar);
+      }
+      if (!sync.wait()) goto done;
+      const int lo = l - 1;  // layer whose pre-activation gradient this is
+#pragma unroll 1
+      for (int c0 = 0; c0 < H; c0 += 32) {
+        float v[32];
+        umma::tmem_ld32(lane_addr + uint32_t(c0), v);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          float z[8], d[8];
+          if (valid) unpack8(*reinterpret_cast<const uint4*>(a.save + save_z(a.B, lo) + b * H + c0 + 8 * q), z);
+          else
+#pragma unroll
+            for (int j = 0; j < 8; j++) z[j] = 0.f;
+#pragma unroll
+          for (int j = 0; j < 8; j++) d[j] = valid ? v[8 * q + j] * dsilu(z[j]) : 0.f;
+          const uint4 dv = pack8(d);
+          *reinterpret_cast<uint4*>(s_act + umma::kmaj_off(t, c0 + 8 * q, H)) = dv;
+          if (valid) *reinterpret_cast<uint4*>(a.dz + int64_t(lo) * a.B * H + b * H + c0 + 8 * q) = dv;
+        }
+      }
+      umma::fence_before_sync();
+      umma::fence_async_shared();
+      __syncthreads();
+    }
+  }
+done:
+  teardown(tbase, 128);
+}
+
+// ---------------------------------------------------------------------------
+// Weight gradients: per CTA, chunks of KC batch rows; partial sums [cta][N_PARAM]
+// ---------------------------------------------------------------------------
+struct WgArgs {
+  const __nv_bfloat16* save;
+  const __nv_bfloat16* dz;   // [4][B][128]
+  const __nv_bfloat16* dz4;  // [B][16]
+  int64_t B;
+  float* partial;            // [gridDim.x][N_PARAM]
+  unsigned* status;
+};
+
+constexpr int WG_A = H * KC * 2;      // one [128 x K64] operand
+constexpr int WG_BA = NAUG * KC * 2;  // one [144 x K64] operand
+constexpr int WG_B16 = 16 * KC * 2;   // one [16 x K64] operand
+constexpr int WG_SMEM = 5 * WG_A + 3 * WG_BA + 2 * WG_B16 + 64;
+// TMEM columns of the five accumulators (32-column aligned; 512 allocated)
+constexpr int ACC1 = 0, ACC2 = 160, ACC3 = 320, ACC0 = 480, ACC4 = 496;
+
+// rows [0, 128) of a K-major [rows x K64] tile <- transpose of a [KC][128]
+// row-major BF16 block (rows b0 .. b0+KC of the batch; rows past B are zero)
+__device__ __forceinline__ void stage_t128(uint8_t* dst, const __nv_bfloat16* src, int64_t b0, int64_t B) {
+  const int f = threadIdx.x;  // 128 threads: one output row each
+#pragma unroll 1
+  for (int g = 0; g < KC / 8; g++) {
+    float v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int64_t b = b0 + g * 8 + j;
+      v[j] = b < B ? __bfloat162float(src[b * H + f]) : 0.f;
+    }
+    *reinterpret_cast<uint4*>(dst + umma::kmaj_off(f, g * 8, KC)) = pack8(v);
+  }
+}
+// 16-row version from a [KC][16] block
+__device__ __forceinline__ void stage_t16(uint8_t* dst, const __nv_bfloat16* src, int64_t b0, int64_t B) {
+  const int f = threadIdx.x & 15, g = threadIdx.x >> 4;  // 16 rows x 8 groups
+  float v[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const int64_t b = b0 + g * 8 + j;
+    v[j] = b < B ? __bfloat162float(src[b * 16 + f]) : 0.f;
+  }
+  *reinterpret_cast<uint4*>(dst + umma::kmaj_off(f, g * 8, KC)) = pack8(v);
+}
+
+__global__ void __launch_bounds__(128, 1) mlp_wgrad_kernel(WgArgs a) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  uint8_t* sA[5];  // dZ0^T, dZ1^T, dZ2^T, dZ3^T, H3^T
+  for (int i = 0; i < 5; i++) sA[i] = sm + i * WG_A;
+  uint8_t* sB[3];  // [H0|1]^T, [H1|1]^T, [H2|1]^T
+  for (int i = 0; i < 3; i++) sB[i] = sm + 5 * WG_A + i * WG_BA;
+  uint8_t* sX = sm + 5 * WG_A + 3 * WG_BA;  // X0^T
+  uint8_t* sD4 = sX + WG_B16;                // dZ4^T
+  uint64_t* s_mbar = reinterpret_cast<uint64_t*>(sD4 + WG_B16);
+  uint32_t* s_tslot = reinterpret_cast<uint32_t*>(s_mbar + 1);
+  const int t = threadIdx.x, w = t >> 5;
+  // constant rows of the augmented operands: a row of ones, then zeros
+  for (int i = 0; i < 3; i++)
+    for (int r = H + t / 8; r < NAUG; r += 16) {
+      float v[8];
+      const int g = t % 8;
+#pragma unroll
+      for (int j = 0; j < 8; j++) v[j] = r == H ? 1.f : 0.f;
+      *reinterpret_cast<uint4*>(sB[i] + umma::kmaj_off(r, g * 8, KC)) = pack8(v);
+    }
+  const uint32_t tbase = setup(s_mbar, s_tslot, 512);
+  TileSync sync{umma::smem_addr(s_mbar), 0u, a.status};
+  const uint32_t idA = umma::idesc_bf16(128, NAUG), id16 = umma::idesc_bf16(128, 16);
+  const int64_t n_chunks = (a.B + KC - 1) / KC;
+  float db4 = 0.f;
+  bool first = true;
+  for (int64_t ch = blockIdx.x; ch < n_chunks; ch += gridDim.x) {
+    const int64_t b0 = ch * KC;
+    for (int l = 0; l < 4; l++) stage_t128(sA[l], a.dz + int64_t(l) * a.B * H, b0, a.B);
+    stage_t128(sA[4], a.save + save_h(a.B, 3), b0, a.B);
+    for (int l = 0; l < 3; l++) stage_t128(sB[l], a.save + save_h(a.B, l), b0, a.B);
+    stage_t16(sX, a.save + save_x0(a.B), b0, a.B);
+    stage_t16(sD4, a.dz4, b0, a.B);
+    if (t < 16)
+      for (int j = 0; j < KC; j++) {
+        const int64_t b = b0 + j;
+        if (b < a.B) db4 += __bfloat162float(a.dz4[b * 16 + t]);
+      }
+    umma::fence_async_shared();
+    __syncthreads();
+    if (t == 0) {
+      umma::fence_after_sync();
+#pragma unroll 1
+      for (int s = 0; s < KC / 16; s++) {
+        const uint32_t acc = (first && s == 0) ? 0u : 1u;
+        for (int l = 1; l <= 3; l++)
+          umma::mma_bf16(tbase + uint32_t(l == 1 ? ACC1 : l == 2 ? ACC2 : ACC3),
+                         umma::kmaj_desc(umma::smem_addr(sA[l]), KC, s),
+                         umma::kmaj_desc(umma::smem_addr(sB[l - 1]), KC, s), idA, acc);
+        umma::mma_bf16(tbase + ACC0, umma::kmaj_desc(umma::smem_addr(sA[0]), KC, s),
+                       umma::kmaj_desc(umma::smem_addr(sX), KC, s), id16, acc);
+        umma::mma_bf16(tbase + ACC4, umma::kmaj_desc(umma::smem_addr(sA[4]), KC, s),
+                       umma::kmaj_desc(umma::smem_addr(sD4), KC, s), id16, acc);
+      }
+      umma::commit(sync.mbar);
+    }
+    first = false;
+    if (!sync.wait()) goto done;
+    umma::fence_before_sync();
+    __syncthreads();  // operands consumed before the next chunk overwrites them
+  }
+  {
+    float* P = a.partial + int64_t(blockIdx.x) * N_PARAM;
+    const int row = t;  // TMEM lane of this thread
+    const uint32_t lane_addr = tbase + (uint32_t(w * 32) << 16);
+    if (first) {  // this CTA had no rows
+      for (int i = t; i < N_PARAM; i += blockDim.x) P[i] = 0.f;
+    } else {
+      for (int l = 1; l <= 3; l++) {
+        const uint32_t base = lane_addr + uint32_t(l == 1 ? ACC1 : l == 2 ? ACC2 : ACC3);
+        const int offW = l == 1 ? OFF_W1 : l == 2 ? OFF_W2 : OFF_W3;
+        const int offB = l == 1 ? OFF_B1 : l == 2 ? OFF_B2 : OFF_B3;
+#pragma unroll 1
+        for (int c0 = 0; c0 < H; c0 += 32) {
+          float v[32];
+          umma::tmem_ld32(base + uint32_t(c0), v);
+#pragma unroll
+          for (int j = 0; j < 32; j++) P[offW + row * H + c0 + j] = v[j];
+        }
+        float v[16];
+        umma::tmem_ld16(base + uint32_t(H), v);
+        P[offB + row] = v[0];
+      }
+      float v[16];
+      umma::tmem_ld16(lane_addr + ACC0, v);
+#pragma unroll
+      for (int j = 0; j < 16; j++) P[OFF_W0 + row * KIN + j] = v[j];
+      umma::tmem_ld16(lane_addr + ACC4, v);
+#pragma unroll
+      for (int j = 0; j < 16; j++) P[OFF_W4 + j * H + row] = v[j];
+      if (t < 16) P[OFF_B4 + t] = db4;
+    }
+  }
+done:
+  teardown(tbase, 512);
+}
+
+// ---------------------------------------------------------------------------
+// Gradient reduction, Adam and the BF16 images (one thread per parameter)
+// ---------------------------------------------------------------------------
+struct AdamArgs {
+  const float* partial;
+  int n_part;
+  float* params;
+  float* m;
+  float* v;
+  float* grad;         // summed gradient (written when non-null)
+  uint8_t* img_fwd;
+  uint8_t* img_bwd;
+  const int* step;     // Adam step count including this update
+  float lr;
+  int apply;           // 0: only sum the gradient
+};
+
+__device__ __forceinline__ void write_images(const AdamArgs& a, int p, float w) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(w);
+  auto put = [&](uint8_t* img, int off, int r, int k, int K) {
+    *reinterpret_cast<__nv_bfloat16*>(img + off + umma::kmaj_off(r, k, K)) = h;
+  };
+  if (p < OFF_W1) {
+    const int o = (p - OFF_W0) / KIN, i = (p - OFF_W0) % KIN;
+    put(a.img_fwd, IMG_W0, o, i, KIN);
+  } else if (p < OFF_B1) {
+    const int l = (p - OFF_W1) / (H * H), e = (p - OFF_W1) % (H * H), o = e / H, i = e % H;
+    put(a.img_fwd, IMG_W1 + l * H * H * 2, o, i, H);
+    put(a.img_bwd, IMG_T1 + l * H * H * 2, i, o, H);
+  } else if (p >= OFF_W4 && p < OFF_B4) {
+    const int o = (p - OFF_W4) / H, i = (p - OFF_W4) % H;
+    put(a.img_fwd, IMG_W4, o, i, H);
+    put(a.img_bwd, IMG_T4, i, o, NOUT);
+  }
+}
+
+__global__ void mlp_adam_kernel(AdamArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N_PARAM) return;
+  float g = 0.f;
+  for (int c = 0; c < a.n_part; c++) g += a.partial[int64_t(c) * N_PARAM + p];
+  if (a.grad) a.grad[p] = g;
+  if (!a.apply) return;
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const int t = max(*a.step, 1);  // advanced by mlp_step_kernel before this update
+  const float m = b1 * a.m[p] + (1.f - b1) * g;
+  const float v = b2 * a.v[p] + (1.f - b2) * g * g;
+  a.m[p] = m;
+  a.v[p] = v;
+  const float mh = m / (1.f - powf(b1, float(t)));
+  const float vh = v / (1.f - powf(b2, float(t)));
+  const float w = a.params[p] - a.lr * mh / (sqrtf(vh) + eps);
+  a.params[p] = w;
+  write_images(a, p, w);
+}
+
+__global__ void mlp_images_kernel(AdamArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < N_PARAM) write_images(a, p, a.params[p]);
+}
+
+__global__ void mlp_step_kernel(int* step, double* loss) {
+  *step += 1;
+  *loss = 0.0;
+}
+
+// uniform sample indices in [0, n) from a counter-based hash (splitmix64)
+__global__ void mlp_sample_kernel(int64_t* idx, int64_t B, int64_t n, uint64_t seed, const int* step) {
+  const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  uint64_t z = seed + 0x9E3779B97F4A7C15ull * (uint64_t(*step) * uint64_t(B) + uint64_t(b) + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  idx[b] = int64_t(z % uint64_t(n));
+}
+
+// One GEMM D[128 x N] = A[128 x K] B[N x K]^T through the same tcgen05 path
+// (operands row-major BF16 in global memory), for testing the descriptors.
+__global__ void __launch_bounds__(128, 1) umma_gemm_test_kernel(const __nv_bfloat16* A, const __nv_bfloat16* B,
+                                                               int N, int K, float* D, unsigned* status) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  uint8_t* sa = sm;
+  uint8_t* sb = sm + 128 * K * 2;
+  uint64_t* s_mbar = reinterpret_cast<uint64_t*>(sb + N * K * 2);
+  uint32_t* s_tslot = reinterpret_cast<uint32_t*>(s_mbar + 1);
+  const int t = threadIdx.x, w = t >> 5;
+  for (int i = t; i < 128 * K; i += blockDim.x)
+    *reinterpret_cast<__nv_bfloat16*>(sa + umma::kmaj_off(i / K, i % K, K)) = A[i];
+  for (int i = t; i < N * K; i += blockDim.x)
+    *reinterpret_cast<__nv_bfloat16*>(sb + umma::kmaj_off(i / K, i % K, K)) = B[i];
+  const uint32_t tbase = setup(s_mbar, s_tslot, 256);
+  TileSync sync{umma::smem_addr(s_mbar), 0u, status};
+  umma::fence_async_shared();
+  __syncthreads();
+  if (t == 0) {
+    umma::fence_after_sync();
+    for (int s = 0; s < K / 16; s++)
+      umma::mma_bf16(tbase, umma::kmaj_desc(umma::smem_addr(sa), K, s), umma::kmaj_desc(umma::smem_addr(sb), K, s),
+                     umma::idesc_bf16(128, N), s > 0 ? 1u : 0u);
+    umma::commit(sync.mbar);
+  }
+  if (sync.wait()) {
+    for (int c0 = 0; c0 < N; c0 += 16) {
+      float v[16];
+      umma::tmem_ld16(tbase + (uint32_t(w * 32) << 16) + uint32_t(c0), v);
+      for (int j = 0; j < 16; j++) D[t * N + c0 + j] = v[j];
+    }
+  }
+  teardown(tbase, 256);
+}
+
+}  // namespace mlp
+}  // namespace nf
+
+// ---------------------------------------------------------------------------
+// Host object and C ABI
+// ---------------------------------------------------------------------------
+using namespace nf::mlp;
+
+namespace {
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+struct Buf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    if (count <= n) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    ck(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+    n = count;
+  }
+  ~Buf() {
+    if (p) cudaFree(p);
+  }
+};
+
+std::string g_mlp_error;
+
+}  // namespace
+
+struct nf_mlp {
+  cudaStream_t stream = nullptr;
+  int n_sm = 148;
+  Buf<float> params, m, v, grad, partial, feat, target, out;
+  Buf<uint8_t> img_fwd, img_bwd;
+  Buf<int> step;
+  Buf<double> loss;
+  Buf<unsigned> status;
+  Buf<int64_t> idx;
+  Buf<__nv_bfloat16> save, dz, dz4;
+  int64_t n_data = 0;
+  int64_t batch = 0;
+  int n_wg = 0;
+  cudaGraphExec_t graph = nullptr;
+  int64_t graph_batch = 0;
+  uint64_t graph_seed = 0;
+  float graph_lr = 0.f;
+  std::string err;
+
+  int64_t ensured = 0;
+  void ensure_batch(int64_t B) {
+    if (B != ensured && graph) {  // the captured step holds this batch's buffers
+      cudaGraphExecDestroy(graph);
+      graph = nullptr;
+    }
+    ensured = B;
+    save.alloc(size_t(save_size(B)));
+    dz.alloc(size_t(4) * B * H);
+    dz4.alloc(size_t(B) * NOUT);
+    idx.alloc(size_t(B));
+    n_wg = int(std::min<int64_t>(n_sm, (B + KC - 1) / KC));
+    partial.alloc(size_t(n_wg) * N_PARAM);
+  }
+  AdamArgs adam_args(float lr, int apply) {
+    AdamArgs a{};
+    a.partial = partial.p;
+    a.n_part = n_wg;
+    a.params = params.p;
+    a.m = m.p;
+    a.v = v.p;
+    a.grad = grad.p;
+    a.img_fwd = img_fwd.p;
+    a.img_bwd = img_bwd.p;
+    a.step = step.p;
+    a.lr = lr;
+    a.apply = apply;
+    return a;
+  }
+  // forward (+ loss gradient), backward, weight gradients, reduction (+ Adam)
+  void enqueue_pass(const float* f, const float* tg, const int64_t* ix, int64_t B, float lr, int apply) {
+    FwdArgs fa{};
+    fa.img = img_fwd.p;
+    fa.params = params.p;
+    fa.feat = f;
+    fa.target = tg;
+    fa.idx = ix;
+    fa.B = B;
+    fa.save = save.p;
+    fa.dz4 = dz4.p;
+    fa.loss = loss.p;
+    fa.loss_scale = 2.0f / float(B * NO);
+    fa.status = status.p;
+    const int n_tiles = int((B + TILE - 1) / TILE);
+    mlp_forward_kernel<<<std::min(n_tiles, n_sm), 128, FWD_SMEM, stream>>>(fa);
+    BwdArgs ba{img_bwd.p, save.p, dz4.p, B, dz.p, status.p};
+    mlp_backward_kernel<<<std::min(n_tiles, n_sm), 128, BWD_SMEM, stream>>>(ba);
+    WgArgs wa{save.p, dz.p, dz4.p, B, partial.p, status.p};
+    mlp_wgrad_kernel<<<n_wg, 128, WG_SMEM, stream>>>(wa);
+    mlp_adam_kernel<<<(N_PARAM + 255) / 256, 256, 0, stream>>>(adam_args(lr, apply));
+  }
+  void check_status() {
+    unsigned st = 0;
+    ck(cudaMemcpyAsync(&st, status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream), "status D2H");
+    ck(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    if (st) throw std::runtime_error("tensor-core wait timed out in an MLP kernel");
+  }
+  ~nf_mlp() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+template <typename F>
+int mlp_guarded(nf_mlp* m, F&& fn) {
+  if (!m) return NF_ERR_ARG;
+  try {
+    return fn();
+  } catch (const std::exception& e) {
+    m->err = e.what();
+    return NF_ERR_CUDA;
+  }
+}
+
+void set_kernel_smem() {
+  ck(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM), "smem attr");
+  ck(cudaFuncSetAttribute(mlp_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, BWD_SMEM), "smem attr");
+  ck(cudaFuncSetAttribute(mlp_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, WG_SMEM), "smem attr");
+  ck(cudaFuncSetAttribute(umma_gemm_test_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024),
+     "smem attr");
+}
+
+}  // namespace
+
+extern "C" {
+
+int nf_mlp_param_count(void) { return N_PARAM; }
+
+nf_mlp* nf_mlp_create(uint64_t seed) {
+  auto m = std::make_unique<nf_mlp>();
+  try {
+    set_kernel_smem();
+    ck(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    int dev = 0;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    ck(cudaDeviceGetAttribute(&m->n_sm, cudaDevAttrMultiProcessorCount, dev), "attr");
+    std::vector<float> p(N_PARAM, 0.f);
+    std::mt19937_64 rng(seed);
+    auto fill = [&](int off, int rows, int cols, int used_rows, int used_cols, int fan_in) {
+      std::uniform_real_distribution<float> u(-1.f / std::sqrt(float(fan_in)), 1.f / std::sqrt(float(fan_in)));
+      for (int r = 0; r < used_rows; r++)
+        for (int c = 0; c < used_cols; c++) p[size_t(off + r * cols + c)] = u(rng);
+      (void)rows;
+    };
+    fill(OFF_W0, H, KIN, H, NIN + 1, NIN);  // weights and the bias column
+    fill(OFF_W1, H, H, H, H, H);
+    fill(OFF_W2, H, H, H, H, H);
+    fill(OFF_W3, H, H, H, H, H);
+    fill(OFF_B1, 1, 3 * H, 1, 3 * H, H);
+    fill(OFF_W4, NOUT, H, NO, H, H);
+    fill(OFF_B4, 1, NOUT, 1, NO, H);
+    m->params.alloc(N_PARAM);
+    m->m.alloc(N_PARAM);
+    m->v.alloc(N_PARAM);
+    m->grad.alloc(N_PARAM);
+    m->img_fwd.alloc(IMG_FWD);
+    m->img_bwd.alloc(IMG_BWD);
+    m->step.alloc(1);
+    m->loss.alloc(1);
+    m->status.alloc(1);
+    ck(cudaMemcpyAsync(m->params.p, p.data(), N_PARAM * sizeof(float), cudaMemcpyHostToDevice, m->stream), "H2D");
+    ck(cudaMemsetAsync(m->m.p, 0, N_PARAM * sizeof(float), m->stream), "memset");
+    ck(cudaMemsetAsync(m->v.p, 0, N_PARAM * sizeof(float), m->stream), "memset");
+    ck(cudaMemsetAsync(m->img_fwd.p, 0, IMG_FWD, m->stream), "memset");
+    ck(cudaMemsetAsync(m->img_bwd.p, 0, IMG_BWD, m->stream), "memset");
+    ck(cudaMemsetAsync(m->step.p, 0, sizeof(int), m->stream), "memset");
+    ck(cudaMemsetAsync(m->loss.p, 0, sizeof(double), m->stream), "memset");
+    ck(cudaMemsetAsync(m->status.p, 0, sizeof(unsigned), m->stream), "memset");
+    mlp_images_kernel<<<(N_PARAM + 255) / 256, 256, 0, m->stream>>>(m->adam_args(0.f, 0));
+    ck(cudaGetLastError(), "images");
+    ck(cudaStreamSynchronize(m->stream), "sync");
+  } catch (const std::exception& e) {
+    g_mlp_error = std::string("nf_mlp_create: ") + e.what();
+    return nullptr;
+  }
+  return m.release();
+}
+
+const char* nf_mlp_last_error(const nf_mlp* m) { return m ? m->err.c_str() : g_mlp_error.c_str(); }
+
+void nf_mlp_destroy(nf_mlp* m) {
+  if (m && m->stream) cudaStreamSynchronize(m->stream);
+  delete m;
+}
+
+int nf_mlp_get_params(nf_mlp* m, float* out) {
+  return mlp_guarded(m, [&]() -> int {
+    if (!out) return NF_ERR_ARG;
+    ck(cudaMemcpyAsync(out, m->params.p, N_PARAM * sizeof(float), cudaMemcpyDeviceToHost, m->stream), "D2H");
+    ck(cudaStreamSynchronize(m->stream), "sync");
+    return NF_OK;
+  });
+}
+
+int nf_mlp_set_params(nf_mlp* m, const float* in) {
+  return mlp_guarded(m, [&]() -> int {
+    if (!in) return NF_ERR_ARG;
+    ck(cudaMemcpyAsync(m->params.p, in, N_PARAM * sizeof(float), cudaMemcpyHostToDevice, m->stream), "H2D");
+    mlp_images_kernel<<<(N_PARAM + 255) / 256, 256, 0, m->stream>>>(m->adam_args(0.f, 0));
+    ck(cudaGetLastError(), "images");
+    ck(cudaStreamSynchronize(m->stream), "sync");
+    return NF_OK;
+  });
+}
+
+int nf_mlp_set_data(nf_mlp* m, const float* features, const float* targets, int64_t n) {
+  return mlp_guarded(m, [&]() -> int {
+    if (!features || !targets || n <= 0) return NF_ERR_ARG;
+    m->feat.alloc(size_t(n) * NIN);
+    m->target.alloc(size_t(n) * NO);
+    ck(cudaMemcpyAsync(m->feat.p, features, size_t(n) * NIN * sizeof(float), cudaMemcpyHostToDevice, m->stream),
+       "H2D");
+    ck(cudaMemcpyAsync(m->target.p, targets, size_t(n) * NO * sizeof(float), cudaMemcpyHostToDevice, m->stream),
+       "H2D");
+    ck(cudaStreamSynchronize(m->stream), "sync");
+    m->n_data = n;
+    return NF_OK;
+  });
+}
+
+int nf_mlp_train(nf_mlp* m, int64_t steps, int64_t batch, float lr, uint64_t seed, int n_report,
+                 double* loss_report, double* ms_out) {
+  return mlp_guarded(m, [&]() -> int {
+    if (steps < 0 || batch <= 0 || m->n_data <= 0 || n_report < 0 || (n_report > 0 && !loss_report))
+      return NF_ERR_ARG;
+    m->ensure_batch(batch);
+    if (!m->graph || m->graph_batch != batch || m->graph_seed != seed || m->graph_lr != lr) {
+      if (m->graph) cudaGraphExecDestroy(m->graph);
+      m->graph = nullptr;
+      cudaGraph_t g = nullptr;
+      ck(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal), "capture");
+      mlp_step_kernel<<<1, 1, 0, m->stream>>>(m->step.p, m->loss.p);  // loss = 0 (step advanced below)
+      mlp_sample_kernel<<<int((batch + 255) / 256), 256, 0, m->stream>>>(m->idx.p, batch, m->n_data, seed, m->step.p);
+      m->enqueue_pass(m->feat.p, m->target.p, m->idx.p, batch, lr, 1);
+      ck(cudaStreamEndCapture(m->stream, &g), "capture");
+      ck(cudaGraphInstantiate(&m->graph, g, 0), "instantiate");
+      cudaGraphDestroy(g);
+      m->graph_batch = batch;
+      m->graph_seed = seed;
+      m->graph_lr = lr;
+    }
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "event");
+    ck(cudaEventCreate(&e1), "event");
+    ck(cudaEventRecord(e0, m->stream), "event");
+    // n_report segments; after each, the mean squared error of its last step
+    int64_t done = 0;
+    for (int r = 0; r < std::max(n_report, 1); r++) {
+      const int64_t upto = n_report > 0 ? steps * (r + 1) / n_report : steps;
+      for (; done < upto; done++) ck(cudaGraphLaunch(m->graph, m->stream), "graph launch");
+      if (n_report > 0) {
+        double l = 0;
+        ck(cudaMemcpyAsync(&l, m->loss.p, sizeof(double), cudaMemcpyDeviceToHost, m->stream), "D2H");
+        ck(cudaStreamSynchronize(m->stream), "sync");
+        loss_report[r] = l / double(batch * NO);
+      }
+    }
+    ck(cudaEventRecord(e1, m->stream), "event");
+    ck(cudaEventSynchronize(e1), "event");
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, e0, e1), "event");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ms_out) *ms_out = ms;
+    m->check_status();
+    return NF_OK;
+  });
+}
+
+int nf_mlp_gradients(nf_mlp* m, const float* features, const float* targets, int64_t n, float* grad_out,
+                     double* loss_out) {
+  return mlp_guarded(m, [&]() -> int {
+    if (!features || !targets || n <= 0 || !grad_out) return NF_ERR_ARG;
+    m->ensure_batch(n);
+    Buf<float> f, tg;
+    f.alloc(size_t(n) * NIN);
+    tg.alloc(size_t(n) * NO);
+    ck(cudaMemcpyAsync(f.p, features, size_t(n) * NIN * sizeof(float), cudaMemcpyHostToDevice, m->stream), "H2D");
+    ck(cudaMemcpyAsync(tg.p, targets, size_t(n) * NO * sizeof(float), cudaMemcpyHostToDevice, m->stream), "H2D");
+    ck(cudaMemsetAsync(m->loss.p, 0, sizeof(double), m->stream), "memset");
+    m->enqueue_pass(f.p, tg.p, nullptr, n, 0.f, 0);
+    ck(cudaGetLastError(), "launch");
+    ck(cudaMemcpyAsync(grad_out, m->grad.p, N_PARAM * sizeof(float), cudaMemcpyDeviceToHost, m->stream), "D2H");
+    double l = 0;
+    ck(cudaMemcpyAsync(&l, m->loss.p, sizeof(double), cudaMemcpyDeviceToHost, m->stream), "D2H");
+    ck(cudaStreamSynchronize(m->stream), "sync");
+    if (loss_out) *loss_out = l / double(n * NO);
+    m->check_status();
+    return NF_OK;
+  });
+}
+
+int nf_mlp_predict(nf_mlp* m, const float* features, int64_t n, float* out, double* ms_out) {
+  return mlp_guarded(m, [&]() -> int {
+    if (!features || !out || n <= 0) return NF_ERR_ARG;
+    Buf<float> f, o;
+    f.alloc(size_t(n) * NIN);
+    o.alloc(size_t(n) * NO);
+    ck(cudaMemcpyAsync(f.p, features, size_t(n) * NIN * sizeof(float), cudaMemcpyHostToDevice, m->stream), "H2D");
+    FwdArgs fa{};
+    fa.img = m->img_fwd.p;
+    fa.params = m->params.p;
+    fa.feat = f.p;
+    fa.B = n;
+    fa.out = o.p;
+    fa.status = m->status.p;
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "event");
+    ck(cudaEventCreate(&e1), "event");
+    ck(cudaEventRecord(e0, m->stream), "event");
+    const int n_tiles = int((n + TILE - 1) / TILE);
+    mlp_forward_kernel<<<std::min(n_tiles, m->n_sm), 128, FWD_SMEM, m->stream>>>(fa);
+    ck(cudaGetLastError(), "launch");
+    ck(cudaEventRecord(e1, m->stream), "event");
+    ck(cudaMemcpyAsync(out, o.p, size_t(n) * NO * sizeof(float), cudaMemcpyDeviceToHost, m->stream), "D2H");
+    ck(cudaStreamSynchronize(m->stream), "sync");
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, e0, e1), "event");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ms_out) *ms_out = ms;
+    m->check_status();
+    return NF_OK;
+  });
+}
+
+int nf_mlp_gemm_selftest(const uint16_t* A, const uint16_t* B, int N, int K, float* D) {
+  if (!A || !B || !D || N < 16 || N > 256 || N % 16 || K < 16 || K > 256 || K % 16) return NF_ERR_ARG;
+  try {
+    set_kernel_smem();
+    Buf<__nv_bfloat16> a, b;
+    Buf<float> d;
+    Buf<unsigned> st;
+    a.alloc(size_t(128) * K);
+    b.alloc(size_t(N) * K);
+    d.alloc(size_t(128) * N);
+    st.alloc(1);
+    ck(cudaMemcpy(a.p, A, size_t(128) * K * 2, cudaMemcpyHostToDevice), "H2D");
+    ck(cudaMemcpy(b.p, B, size_t(N) * K * 2, cudaMemcpyHostToDevice), "H2D");
+    ck(cudaMemset(st.p, 0, sizeof(unsigned)), "memset");
+    const int smem = (128 + N) * K * 2 + 64;
+    umma_gemm_test_kernel<<<1, 128, smem>>>(a.p, b.p, N, K, d.p, st.p);
+    ck(cudaGetLastError(), "launch");
+    ck(cudaDeviceSynchronize(), "sync");
+    unsigned s = 0;
+    ck(cudaMemcpy(&s, st.p, sizeof(unsigned), cudaMemcpyDeviceToHost), "D2H");
+    if (s) throw std::runtime_error("tensor-core wait timed out");
+    ck(cudaMemcpy(D, d.p, size_t(128) * N * 4, cudaMemcpyDeviceToHost), "D2H");
+  } catch (const std::exception& e) {
+    g_mlp_error = e.what();
+    return NF_ERR_CUDA;
+  }
+  return NF_OK;
+}
+
+}  // extern "C"

@@ -1137,14 +1137,18 @@ static void enqueue_residual(nf_solver* s) {
                                                                           s->res_out.p);
 }
 
-int nf_solve_steady(nf_solver* s, double tol, int64_t max_steps, int check_every, int64_t* steps_per_case,
-                    double* res0_per_case, double* res_per_case, double* ms_per_case) {
+namespace {
+
+// tol > 0: relative to each case's first residual; else abs_target[case].
+int solve_steady_impl(nf_solver* s, double tol, const double* abs_target, int64_t max_steps, int check_every,
+                      int64_t* steps_per_case, double* res0_per_case, double* res_per_case, double* ms_per_case) {
   return guarded(s, [&]() -> int {
     if (!s->p.local_time_stepping) {
       s->err = "nf_solve_steady needs local time stepping";
       return NF_ERR_ARG;
     }
-    if (!(tol > 0.0) || max_steps < 1 || check_every < 1) return NF_ERR_ARG;
+    if (!(tol > 0.0) && !abs_target) return NF_ERR_ARG;
+    if (max_steps < 1 || check_every < 1) return NF_ERR_ARG;
     const int nc = s->n_cases;
     std::vector<int> frozen(size_t(nc), 0);
     std::vector<int64_t> steps(size_t(nc), -1);
@@ -1190,10 +1194,12 @@ int nf_solve_steady(nf_solver* s, double tol, int64_t max_steps, int check_every
     s->run_steps(1);
     read_res();
     int64_t done = 1, left = nc;
+    std::vector<double> target(size_t(nc), 0.0);
     for (int cs = 0; cs < nc; cs++) {
       r0[size_t(cs)] = h[size_t(2 * cs)];
       rl[size_t(cs)] = r0[size_t(cs)];
-      if (!(r0[size_t(cs)] > 0.0)) {  // already steady
+      target[size_t(cs)] = abs_target ? abs_target[cs] : tol * r0[size_t(cs)];
+      if (!(r0[size_t(cs)] > 0.0) || r0[size_t(cs)] <= target[size_t(cs)]) {  // already steady
         steps[size_t(cs)] = 1;
         frozen[size_t(cs)] = 1;
         left--;
@@ -1219,7 +1225,7 @@ int nf_solve_steady(nf_solver* s, double tol, int64_t max_steps, int check_every
         if (s->ratchet_alloc && s->p.limiter_ratchet_drop > 0.0 && !s->h_ratchet[size_t(cs)] &&
             rl[size_t(cs)] <= s->p.limiter_ratchet_drop * r0[size_t(cs)])
           s->ratchet_start(cs);
-        if (rl[size_t(cs)] <= tol * r0[size_t(cs)]) {
+        if (rl[size_t(cs)] <= target[size_t(cs)]) {
           frozen[size_t(cs)] = 1;
           steps[size_t(cs)] = done;
           ms[size_t(cs)] = t;
@@ -1239,6 +1245,22 @@ int nf_solve_steady(nf_solver* s, double tol, int64_t max_steps, int check_every
     }
     return s->check_status();
   });
+}
+
+}  // namespace
+
+int nf_solve_steady(nf_solver* s, double tol, int64_t max_steps, int check_every, int64_t* steps_per_case,
+                    double* res0_per_case, double* res_per_case, double* ms_per_case) {
+  if (!(tol > 0.0)) return NF_ERR_ARG;
+  return solve_steady_impl(s, tol, nullptr, max_steps, check_every, steps_per_case, res0_per_case, res_per_case,
+                           ms_per_case);
+}
+
+int nf_solve_steady_to(nf_solver* s, const double* res_target, int64_t max_steps, int check_every,
+                       int64_t* steps_per_case, double* res0_per_case, double* res_per_case, double* ms_per_case) {
+  if (!res_target) return NF_ERR_ARG;
+  return solve_steady_impl(s, 0.0, res_target, max_steps, check_every, steps_per_case, res0_per_case, res_per_case,
+                           ms_per_case);
 }
 
 int nf_get_residual(nf_solver* s, double* out, int n_cases) {

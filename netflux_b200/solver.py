@@ -325,6 +325,16 @@ class EulerSolver:
         # the library returns -(steps run) for a case that did not reach tol
         return {"steps": np.abs(steps), "converged": steps > 0, "res0": r0, "res": r1, "ms": ms}
 
+    def solve_steady_to(self, res_target, max_steps: int = 100000, check_every: int = 50) -> dict:
+        """Steady solve to an absolute density residual per case (see nf_solve_steady_to)."""
+        nc = self.mesh.n_cases
+        tgt = np.ascontiguousarray(np.broadcast_to(np.asarray(res_target, np.float64), (nc,)))
+        steps = np.zeros(nc, np.int64)
+        r0, r1, ms = np.zeros(nc), np.zeros(nc), np.zeros(nc)
+        _check(L.load().nf_solve_steady_to(self._h, L.dptr(tgt), int(max_steps), int(check_every), L.i64ptr(steps),
+                                            L.dptr(r0), L.dptr(r1), L.dptr(ms)), self._h)
+        return {"steps": np.abs(steps), "converged": steps > 0, "res0": r0, "res": r1, "ms": ms}
+
     def synchronize(self) -> None:
         _check(L.load().nf_synchronize(self._h), self._h)
 

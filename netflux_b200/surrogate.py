@@ -1,0 +1,243 @@
+"""Surrogate warm start for steady bump-channel solves (extension; the
+reference has no learned part).
+
+An MLP (cell centroid, wall distance, Mach number, bump height -> the five
+conserved variables normalised by the free stream) is trained with the
+library's tensor-core kernels on converged steady solutions produced by the
+solver itself, and is used only as the initial state of a local-time-stepping
+steady solve. The free-stream start is the fallback: it is taken when the
+warm start's first residual exceeds the free-stream one, or when the
+warm-started solve does not reach the target within its step budget. Both
+solves stop at the same absolute residual (the tolerance times the residual
+of the free-stream start), so their final states are comparable.
+"""
+from typing import Dict, Optional, Sequence
+
+import ctypes as C
+import numpy as np
+
+from . import _lib as L
+from . import meshgen as mg
+from . import solver as S
+
+GAMMA = 1.4
+# input ranges mapped to [-1, 1]: x, y, z, wall distance, Mach, bump height
+FEATURE_LO = np.array([0.0, 0.0, 0.0, 0.0, 0.3, 0.05])
+FEATURE_HI = np.array([3.0, 1.0, 1.0, 0.5, 0.8, 0.15])
+
+
+def _check(rc: int, h) -> None:
+    if rc != L.NF_OK:
+        raise L.NetFluxError(rc, (L.load().nf_mlp_last_error(h) or b"").decode())
+
+
+class MLP:
+    """The library's surrogate network (nf_mlp_*)."""
+
+    def __init__(self, seed: int = 0):
+        self._h = L.load().nf_mlp_create(int(seed))
+        if not self._h:
+            raise L.NetFluxError(L.NF_ERR_CUDA, (L.load().nf_mlp_last_error(None) or b"").decode())
+        self.n_param = L.load().nf_mlp_param_count()
+
+    def get_params(self) -> np.ndarray:
+        p = np.empty(self.n_param, np.float32)
+        _check(L.load().nf_mlp_get_params(self._h, L.fptr(p)), self._h)
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.shape == (self.n_param,)
+        _check(L.load().nf_mlp_set_params(self._h, L.fptr(p)), self._h)
+
+    def set_data(self, features: np.ndarray, targets: np.ndarray) -> None:
+        f = np.ascontiguousarray(features, np.float32)
+        t = np.ascontiguousarray(targets, np.float32)
+        assert f.shape[1] == 7 and t.shape == (f.shape[0], 5)
+        _check(L.load().nf_mlp_set_data(self._h, L.fptr(f), L.fptr(t), f.shape[0]), self._h)
+
+    def train(self, steps: int, batch: int = 65536, lr: float = 1e-3, seed: int = 0, n_report: int = 20) -> dict:
+        rep = np.zeros(max(n_report, 1))
+        ms = C.c_double()
+        _check(L.load().nf_mlp_train(self._h, int(steps), int(batch), float(lr), int(seed), int(n_report),
+                                     L.dptr(rep), C.byref(ms)), self._h)
+        return {"loss": rep[:n_report], "ms": ms.value}
+
+    def gradients(self, features: np.ndarray, targets: np.ndarray):
+        f = np.ascontiguousarray(features, np.float32)
+        t = np.ascontiguousarray(targets, np.float32)
+        g = np.empty(self.n_param, np.float32)
+        loss = C.c_double()
+        _check(L.load().nf_mlp_gradients(self._h, L.fptr(f), L.fptr(t), f.shape[0], L.fptr(g), C.byref(loss)),
+               self._h)
+        return loss.value, g
+
+    def predict(self, features: np.ndarray):
+        f = np.ascontiguousarray(features, np.float32)
+        out = np.empty((f.shape[0], 5), np.float32)
+        ms = C.c_double()
+        _check(L.load().nf_mlp_predict(self._h, L.fptr(f), f.shape[0], L.fptr(out), C.byref(ms)), self._h)
+        return out, ms.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.load().nf_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gemm_selftest(A: np.ndarray, B: np.ndarray) -> np.ndarray:
+    """D = A B^T through the tcgen05 path; A [128][K], B [N][K] as BF16 bit patterns (uint16)."""
+    A = np.ascontiguousarray(A, np.uint16)
+    B = np.ascontiguousarray(B, np.uint16)
+    N, K = B.shape
+    D = np.empty((128, N), np.float32)
+    rc = L.load().nf_mlp_gemm_selftest(A.ctypes.data_as(C.POINTER(C.c_uint16)),
+                                        B.ctypes.data_as(C.POINTER(C.c_uint16)), N, K, L.fptr(D))
+    _check(rc, None)
+    return D
+
+
+# ---------------------------------------------------------------------------
+# features and targets
+# ---------------------------------------------------------------------------
+def wall_distance(mesh: S.Mesh, grid: Optional[Dict[str, np.ndarray]] = None) -> np.ndarray:
+    """Distance of every cell centroid to the nearest wall-face centroid (slip and no-slip patches)."""
+    from scipy.spatial import cKDTree
+    g = grid if grid is not None else mesh.export()
+    N = mesh.n_cells
+    pts = []
+    for p in mesh.patches():
+        if p["type"] in (mg.BC_CODES["SlipWall"], mg.BC_CODES["NoSlipWall"]):
+            f = np.arange(p["first_face"], p["first_face"] + p["n_faces"])
+            i = g["face_ij"][f, 0].astype(np.int64)
+            pts.append(g["centroid"][i] + g["ri"][f])
+    if not pts:
+        return np.full(N, FEATURE_HI[3])
+    d, _ = cKDTree(np.concatenate(pts)).query(g["centroid"][:N])
+    return d
+
+
+def features(centroids: np.ndarray, wall_dist: np.ndarray, mach: float, h: float) -> np.ndarray:
+    n = centroids.shape[0]
+    raw = np.column_stack([centroids, wall_dist, np.full(n, mach), np.full(n, h)])
+    return (2.0 * (raw - FEATURE_LO) / (FEATURE_HI - FEATURE_LO) - 1.0).astype(np.float32)
+
+
+def _scales(fs: Sequence[float]):
+    rho, u, v, w, p = fs
+    V = float(np.sqrt(u * u + v * v + w * w))
+    E = p / (GAMMA - 1.0) + 0.5 * rho * V * V
+    base = np.array([1.0, u / V, v / V, w / V, 1.0])
+    scale = np.array([rho, rho * V, rho * V, rho * V, E])
+    return base, scale
+
+
+def normalise_state(U: np.ndarray, fs: Sequence[float]) -> np.ndarray:
+    """Conserved variables divided by the free stream (rho, rho V, E), minus the free stream."""
+    base, scale = _scales(fs)
+    return (U / scale - base).astype(np.float32)
+
+
+def denormalise_state(Y: np.ndarray, fs: Sequence[float]) -> np.ndarray:
+    base, scale = _scales(fs)
+    U = (np.asarray(Y, np.float64) + base) * scale
+    # keep the state physical: density and pressure at least 20% of the free stream
+    rho_min = 0.2 * fs[0]
+    U[:, 0] = np.maximum(U[:, 0], rho_min)
+    ke = 0.5 * (U[:, 1] ** 2 + U[:, 2] ** 2 + U[:, 3] ** 2) / U[:, 0]
+    U[:, 4] = np.maximum(U[:, 4], ke + 0.2 * fs[4] / (GAMMA - 1.0))
+    return U
+
+
+def case_features(mesh: S.Mesh, mach: float, h: float) -> np.ndarray:
+    g = mesh.export()
+    return features(g["centroid"][: mesh.n_cells], wall_distance(mesh, g), mach, h)
+
+
+# ---------------------------------------------------------------------------
+# steady solves
+# ---------------------------------------------------------------------------
+def steady_config(fs: Sequence[float], precision: str = "mixed", limiter: str = "NONE") -> S.Config:
+    return S.Config(precision=precision, CFL=0.8, local_time_stepping=True, limiter=limiter, density_fs=fs[0],
+                    velocity_fs=list(fs[1:4]), pressure_fs=fs[4])
+
+
+def first_residual(solver: S.EulerSolver, U0: np.ndarray) -> float:
+    """Density residual of one step from U0 (the solver is left at U0)."""
+    solver.set_state(U0)
+    solver.advance(1)
+    r = float(solver.residual()[0][0])
+    solver.set_state(U0)
+    return r
+
+
+def solve_plain(mesh: S.Mesh, fs, tol: float = 1e-6, precision: str = "mixed", max_steps: int = 400000,
+                check_every: int = 100) -> dict:
+    cfg = steady_config(fs, precision)
+    s = S.EulerSolver(cfg, mesh, U0=mg.uniform_state(mesh.n_cells, fs))
+    s.tune()
+    U_fs = mg.uniform_state(mesh.n_cells, fs)
+    r_fs = first_residual(s, U_fs)
+    out = s.solve_steady_to(tol * r_fs, max_steps, check_every)
+    res = {"steps": int(out["steps"][0]), "converged": bool(out["converged"][0]), "ms": float(out["ms"][0]),
+           "res_fs": r_fs, "res_final": float(out["res"][0]), "U": s.get_solver_data().get_solution()}
+    s.close()
+    return res
+
+
+def solve_warm(mesh: S.Mesh, fs, mlp: MLP, mach: float, h: float, tol: float = 1e-6, precision: str = "mixed",
+               max_steps: int = 400000, check_every: int = 100, feats: Optional[np.ndarray] = None) -> dict:
+    """Warm-started steady solve with the free-stream fallback."""
+    import time
+    t0 = time.perf_counter()
+    f = case_features(mesh, mach, h) if feats is None else feats
+    Y, ms_mlp = mlp.predict(f)
+    U_w = denormalise_state(Y, fs)
+    t_prep = time.perf_counter() - t0
+    cfg = steady_config(fs, precision)
+    s = S.EulerSolver(cfg, mesh, U0=U_w)
+    s.tune()
+    U_fs = mg.uniform_state(mesh.n_cells, fs)
+    r_fs = first_residual(s, U_fs)
+    r_w = first_residual(s, U_w)
+    fallback = None
+    if not (r_w <= r_fs):
+        fallback = "initial residual above the free-stream start"
+    out = None
+    if fallback is None:
+        out = s.solve_steady_to(tol * r_fs, max_steps, check_every)
+        if not out["converged"][0]:
+            fallback = "warm-started solve did not reach the target"
+    ms_warm = float(out["ms"][0]) if out is not None else 0.0
+    steps_warm = int(out["steps"][0]) if out is not None else 0
+    if fallback is not None:
+        s.set_state(U_fs)
+        out2 = s.solve_steady_to(tol * r_fs, max_steps, check_every)
+        out = {k: v for k, v in out2.items()}
+        steps = steps_warm + int(out2["steps"][0])
+        ms = ms_warm + float(out2["ms"][0])
+    else:
+        steps, ms = steps_warm, ms_warm
+    res = {"steps": steps, "converged": bool(out["converged"][0]), "ms": ms, "ms_mlp": ms_mlp,
+           "prep_s": t_prep, "res_fs": r_fs, "res_warm0": r_w, "res_final": float(out["res"][0]),
+           "fallback": fallback, "U": s.get_solver_data().get_solution(), "U_warm": U_w}
+    s.close()
+    return res
+
+
+def training_set(cases, precision: str = "mixed", tol: float = 1e-6, max_steps: int = 400000):
+    """Converged solutions of (mesh, fs, mach, h) cases -> features, targets and per-case records."""
+    F, T, recs = [], [], []
+    for mesh, fs, mach, h in cases:
+        r = solve_plain(mesh, fs, tol, precision, max_steps)
+        f = case_features(mesh, mach, h)
+        F.append(f)
+        T.append(normalise_state(r["U"], fs))
+        recs.append({k: v for k, v in r.items() if k != "U"})
+    return np.concatenate(F), np.concatenate(T), recs
