@@ -95,6 +95,9 @@ struct StageArgs {
   double* vg;
   double* fb;
   float* fb32;
+  // converged cases of a steady solve (null: none); their cells are skipped
+  // by the fast kernels (cases share no faces, and U is left untouched)
+  const int* case_frozen;
   // limiter ratchet (extension): per-cell case, per-case switch (null: off)
   // and the kept limiter values [5][stride] (FP64 or FP32 with the state form)
   const int* cell_case;
@@ -106,6 +109,9 @@ struct StageArgs {
 // Once a case's ratchet is on, a cell's limiter value is the minimum of the
 // live value and the kept one, and is kept: it only tightens, so it settles
 // and the steady residual can converge (the live Barth limiter makes it stall).
+__device__ __forceinline__ bool frozen_cell(const StageArgs& a, int c) {
+  return a.case_frozen != nullptr && a.case_frozen[a.cell_case[c]] != 0;
+}
 __device__ __forceinline__ bool ratchet_on(const StageArgs& a, int c) {
   return a.lim_ratchet != nullptr && a.lim_ratchet[a.cell_case[c]] != 0;
 }
@@ -456,7 +462,7 @@ __device__ __forceinline__ void face_normals(const T P[4][3], T S[4][3]) {
 template <typename T, bool kPipe, int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView<T> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= m.n) return;
+  if (c >= m.n || frozen_cell(a, c)) return;
   const int st = m.stride;
   static_assert(sizeof(T) == 8, "FP64 kernel");
   const T* Vin = a.Vin;
@@ -599,7 +605,7 @@ __device__ __forceinline__ void stage_update(const StageArgs& a, int c, int st, 
 template <typename T, bool kPipe, int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= m.n) return;
+  if (c >= m.n || frozen_cell(a, c)) return;
   const int st = m.stride;
   const bool second = a.second_order != 0;
   static_assert(sizeof(T) == 8, "FP64 kernel");

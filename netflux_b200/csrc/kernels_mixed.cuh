@@ -75,7 +75,7 @@ __device__ __forceinline__ void rusanov_delta(const float vc[5], const float dL[
 template <bool kPipe, int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshView<float> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= m.n) return;
+  if (c >= m.n || frozen_cell(a, c)) return;
   const int st = m.stride;
   const double* __restrict__ V = a.Vin;
   const double* __restrict__ Vg = a.vg;
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshVie
 template <bool kPipe, int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) flux_delta_kernel(MeshView<float> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= m.n) return;
+  if (c >= m.n || frozen_cell(a, c)) return;
   const int st = m.stride;
   const bool second = a.second_order != 0;
   const double* __restrict__ V = a.Vin;

@@ -254,6 +254,14 @@ struct nf_solver {
     prof_end();
   }
 
+  // primitives of U in both V buffers (as after nf_set_state)
+  void refresh_primitives() {
+    for (int b = 0; b < 2; b++) {
+      if (p.precision == NF_PREC_FP64_REF) nf::launch_prim_ref(n, stride, U.p, Vbuf(b), nullptr, launch());
+      else nf::launch_prim_fast(n, stride, U.p, Vbuf(b), nullptr, launch());
+    }
+  }
+
   void ratchet_reset() {
     ratchet_step_done = false;
     if (!ratchet_alloc) return;
@@ -426,6 +434,8 @@ struct nf_solver {
       a.stage = s;
       a.local_dt = p.local_time_stepping;
       a.freeze = freeze && p.local_time_stepping;
+      a.cell_case = cell_case.p;
+      if (a.freeze && p.precision != NF_PREC_FP64_REF) a.case_frozen = case_frozen.p;
       a.Vin = Vbuf(vcur);
       a.Vout = Vbuf(1 - vcur);
       a.fs = fs.p;
@@ -440,7 +450,6 @@ struct nf_solver {
       a.scal = scal.p;
       a.status = status.p;
       if (ratchet_alloc) {
-        a.cell_case = cell_case.p;
         a.lim_ratchet = case_ratchet.p;
         a.phi_keep = phi_keep.p;
         a.phi_keep32 = phi_keep32.p;
@@ -1175,6 +1184,8 @@ int solve_steady_impl(nf_solver* s, double tol, const double* abs_target, int64_
         s->freeze = false;
         drop();
         cudaMemsetAsync(s->case_frozen.p, 0, size_t(nc) * sizeof(int), s->stream);
+        // frozen cells were skipped: both primitive buffers from U again
+        s->refresh_primitives();
       }
     } restore{s, nc, &e0, &e1, drop_graphs};
     ck(cudaMemsetAsync(s->case_frozen.p, 0, size_t(nc) * sizeof(int), s->stream), "freeze reset");

@@ -1,8 +1,9 @@
 """Surrogate warm start for steady bump-channel solves (extension; the
 reference has no learned part).
 
-An MLP (cell centroid, wall distance, Mach number, bump height -> the five
-conserved variables normalised by the free stream) is trained with the
+An MLP (cell centroid, wall distance, Mach number, bump height and the
+lower-wall height under the cell -> the five conserved variables normalised
+by the free stream) is trained with the
 library's tensor-core kernels on converged steady solutions produced by the
 solver itself, and is used only as the initial state of a local-time-stepping
 steady solve. The free-stream start is the fallback: it is taken when the
@@ -21,9 +22,10 @@ from . import meshgen as mg
 from . import solver as S
 
 GAMMA = 1.4
-# input ranges mapped to [-1, 1]: x, y, z, wall distance, Mach, bump height
-FEATURE_LO = np.array([0.0, 0.0, 0.0, 0.0, 0.3, 0.05])
-FEATURE_HI = np.array([3.0, 1.0, 1.0, 0.5, 0.8, 0.15])
+# input ranges mapped to [-1, 1]: x, y, z, wall distance, Mach, bump height,
+# and the lower-wall height under the cell, h sin^2(pi (x - 1)) on 1 <= x <= 2
+FEATURE_LO = np.array([0.0, 0.0, 0.0, 0.0, 0.3, 0.05, 0.0])
+FEATURE_HI = np.array([3.0, 1.0, 1.0, 0.5, 0.8, 0.15, 0.15])
 
 
 def _check(rc: int, h) -> None:
@@ -125,7 +127,9 @@ def wall_distance(mesh: S.Mesh, grid: Optional[Dict[str, np.ndarray]] = None) ->
 
 def features(centroids: np.ndarray, wall_dist: np.ndarray, mach: float, h: float) -> np.ndarray:
     n = centroids.shape[0]
-    raw = np.column_stack([centroids, wall_dist, np.full(n, mach), np.full(n, h)])
+    x = centroids[:, 0]
+    y_wall = np.where((x >= 1.0) & (x <= 2.0), h * np.sin(np.pi * (x - 1.0)) ** 2, 0.0)
+    raw = np.column_stack([centroids, wall_dist, np.full(n, mach), np.full(n, h), y_wall])
     return (2.0 * (raw - FEATURE_LO) / (FEATURE_HI - FEATURE_LO) - 1.0).astype(np.float32)
 
 

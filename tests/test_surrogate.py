@@ -73,3 +73,31 @@ def test_mlp_training_fits_a_smooth_field():
     r = m.train(600, batch=4096, lr=1e-3, n_report=6)
     print("loss", r0["loss"], r["loss"], "ms", r["ms"])
     assert r["loss"][-1] <= 0.05 * r0["loss"][0]
+
+
+def test_warm_start_gains_over_free_stream_start():
+    """Train on batched steady solutions of small channels, then warm-start a held-out (Mach, h):
+    it reaches the same absolute residual in fewer steps and lands on the plain solve's state."""
+    from netflux_b200 import sweep as SW
+    from netflux_b200 import surrogate as sur
+    from netflux_b200 import meshgen as mg
+    cases = SW.sample_cases(8, 11, 12, 16, (0.35, 0.55), (0.05, 0.1))
+    res = SW.run_batched(cases, "mixed", 1e-6, 100000, 50)
+    assert all(c["converged"] for c in res["per_case"])
+    F, T = SW.training_data(res, cases)
+    mlp = sur.MLP(seed=1)
+    mlp.set_data(F, T)
+    tr = mlp.train(3000, 16384, 1e-3, seed=1, n_report=3)
+    c = {"nx": 14, "mach": 0.45, "h": 0.08}
+    mesh = SW.case_mesh(c)
+    fs = mg.bump_freestream(c["mach"])
+    plain = sur.solve_plain(mesh, fs, 1e-6, "mixed", 100000, 50)
+    warm = sur.solve_warm(mesh, fs, mlp, c["mach"], c["h"], 1e-6, "mixed", 100000, 50)
+    d = np.linalg.norm(warm["U"] - plain["U"]) / np.linalg.norm(plain["U"])
+    d0 = np.linalg.norm(warm["U_warm"] - plain["U"]) / np.linalg.norm(plain["U"])
+    print("train loss", tr["loss"], "plain steps", plain["steps"], "warm steps", warm["steps"],
+          "warm start L2", d0, "final L2", d, "fallback", warm["fallback"])
+    assert plain["converged"] and warm["converged"] and warm["fallback"] is None
+    assert warm["res_final"] <= 1e-6 * plain["res_fs"]
+    assert warm["steps"] < plain["steps"]
+    assert d <= 1e-5
