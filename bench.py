@@ -143,23 +143,32 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
                       local_dt: bool):
     """Compulsory HBM bytes of one launch of each stage kernel (every datum the
     kernel must read or write, once; neighbours' values are other cells' own
-    values and are not counted again). Fast forms (fp64, mixed):
+    values and are not counted again).
 
-    gradient_node, per cell: V (5 r), 4 vertex ids (16), 4 neighbour ids (16),
-    face code (4), vol (8), writes 4 face states (20 r); plus the node array
-    (4 r per node) and one ghost state per boundary face (5 r).
-    flux_node, per cell: 4 own face states (20 r), 4 neighbour face ids (16),
-    face code (4), 4 vertex ids (16), U (40), U^n (40 at stages 2 and 3: 2/3
-    on average), vol (8), local dt (8 with local time stepping), writes U and
-    V (80, plus 20 for the FP32 copy in mixed precision) and R_rho/vol at the
-    first stage (8, 1/3 on average); plus the node array and one boundary flux
-    per boundary face (5 r).
-    r = 8 bytes (fp64) or 4 (mixed) for face work; U, V, vol, dt are FP64.
+    FP64 (gradient_node / flux_node), per cell:
+      gradient: V (40), 4 vertex ids (16), 4 neighbour ids (16), face code (4),
+        vol (8), writes 4 face states (160); per node 32 (xyz + pad); per
+        boundary face one ghost state (40).
+      flux: 4 own face states (160), 4 neighbour face ids (16), face code (4),
+        4 vertex ids (16), U (40), U^n (40 at stages 2 and 3: 2/3 on average),
+        vol (8), local dt (8 with local time stepping), writes U and V (80) and
+        R_rho/vol at the first stage (8, 1/3 on average); per node 32; per
+        boundary face one boundary flux (40).
+    Mixed (gradient_delta / flux_delta, FP32 differences to FP64 state):
+      gradient: V (40), ids (32), code (4), vol (8), writes 4 FP32 increments
+        (80); per node 16; per boundary face an FP64 ghost (40).
+      flux: own V (40), own increments (80), neighbour face ids (16), code (4),
+        vertex ids (16), U, U^n, vol, dt, writes U, V and R_rho as above; per
+        node 16; per boundary face an FP32 flux difference (20).
     """
-    r = 4 if precision == "mixed" else 8
-    grad = n_cells * (5 * r + 16 + 16 + 4 + 8 + 20 * r) + n_nodes * 4 * r + n_boundary * 5 * r
-    flux = n_cells * (20 * r + 16 + 4 + 16 + 40 + 40 * 2 / 3 + 8 + (8 if local_dt else 0) + 80
-                      + (20 if precision == "mixed" else 0) + 8 / 3) + n_nodes * 4 * r + n_boundary * 5 * r
+    lts = 8 if local_dt else 0
+    upd = 40 + 40 * 2 / 3 + 8 + lts + 80 + 8 / 3  # U, U^n, vol, dt, U and V out, R_rho
+    if precision == "mixed":
+        grad = n_cells * (40 + 16 + 16 + 4 + 8 + 80) + n_nodes * 16 + n_boundary * 40
+        flux = n_cells * (40 + 80 + 16 + 4 + 16 + upd) + n_nodes * 16 + n_boundary * 20
+    else:
+        grad = n_cells * (40 + 16 + 16 + 4 + 8 + 160) + n_nodes * 32 + n_boundary * 40
+        flux = n_cells * (160 + 16 + 4 + 16 + upd) + n_nodes * 32 + n_boundary * 40
     return {"flux": flux, "gradient": grad}
 
 

@@ -172,6 +172,11 @@ typedef struct {
    * limiter_ratchet_drop (> 0). Both 0: off. */
   int64_t limiter_ratchet_step;
   double limiter_ratchet_drop;
+  /* Extension: 1 gives far-field ghosts the isentropic density
+   * (c_b^2 / (gamma s_b))^(1/(gamma-1)); 0 (default) keeps the reference's
+   * inverted form (Numerics.cpp:149), which is exact only for a free-stream
+   * density of 1. */
+  int farfield_density_fix;
 } nf_params;
 
 void nf_params_default(nf_params* p);

@@ -56,7 +56,8 @@ class NfParams(C.Structure):
                 ("cfl", C.c_double), ("t_end", C.c_double),
                 ("patches", C.POINTER(NfPatchBC)), ("n_patches", C.c_int),
                 ("freestream", C.c_double * 5), ("block_size", C.c_int), ("kernel_variant", C.c_int),
-                ("limiter_ratchet_step", C.c_int64), ("limiter_ratchet_drop", C.c_double)]
+                ("limiter_ratchet_step", C.c_int64), ("limiter_ratchet_drop", C.c_double),
+                ("farfield_density_fix", C.c_int)]
 
 
 class NetFluxError(RuntimeError):

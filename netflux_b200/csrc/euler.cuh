@@ -47,6 +47,8 @@ struct PatchBC {
   double fs[5];     // rho, u, v, w, p of the free stream
   double c_fs;      // sqrt(gamma * p / rho)
   double s_fs;      // p * rho^-gamma
+  int density_fix;  // extension: 1 = physical far-field density (the reference inverts it)
+  int pad;
 };
 
 template <typename T>
@@ -171,7 +173,10 @@ __device__ __forceinline__ void ghost_state(const PatchBC& bc, const T V[5], con
       G[3] = vfs[2] + (vn_fs - vn_b) * n[2];
       s_b = T(bc.s_fs);
     }
-    const T rho_b = pow(gam * s_b / (c_b * c_b), Gas<T>::g1_inv);
+    // Numerics.cpp:149 computes (gamma s / c^2)^(1/(gamma-1)), the inverse of
+    // the isentropic density; it is exact only for rho = 1 (kept by default)
+    const T rho_b = bc.density_fix ? pow(c_b * c_b / (gam * s_b), Gas<T>::g1_inv)
+                                   : pow(gam * s_b / (c_b * c_b), Gas<T>::g1_inv);
     G[0] = rho_b;
     G[4] = c_b * c_b * rho_b / gam;
   } else {  // BC_NoSlipWall

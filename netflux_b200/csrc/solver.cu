@@ -904,6 +904,8 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
       // BC_FarField::BC_FarField (Numerics.cpp:76-84)
       b.c_fs = std::sqrt(nf::Gas<double>::gamma * fs[4] / fs[0]);
       b.s_fs = fs[4] * std::pow(fs[0], -nf::Gas<double>::gamma);
+      b.density_fix = p.farfield_density_fix ? 1 : 0;
+      b.pad = 0;
       if (b.type < 0 || b.type > 2) throw std::runtime_error("bad boundary type");
     }
 

@@ -97,6 +97,8 @@ class Config:
         # limiter ratchet: from this step on / once a case's residual drop reaches this value
         self.limiter_ratchet_step = int(opts.get("limiter_ratchet_step", 0))
         self.limiter_ratchet_drop = float(opts.get("limiter_ratchet_drop", 0.0))
+        # physical far-field ghost density (the reference's is exact only for rho_fs = 1)
+        self.farfield_density_fix = bool(opts.get("farfield_density_fix", False))
         self.delta_time = 0.0
         self.time = 0.0
         self.timestep = 0
@@ -225,6 +227,7 @@ def make_params(config: Config, mesh: Mesh, keep_stage_fields: bool = False,
     p.kernel_variant = int(variant)
     p.limiter_ratchet_step = config.limiter_ratchet_step
     p.limiter_ratchet_drop = config.limiter_ratchet_drop
+    p.farfield_density_fix = int(config.farfield_density_fix)
     for k in range(5):
         p.freestream[k] = config.primvars_inf[k]
     arr = None

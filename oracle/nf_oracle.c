@@ -80,6 +80,8 @@ static void rusanov(const double* UL, const double* UR, const double* S, double*
 }
 
 /* BoundaryCondition::calc_ghost_val (Numerics.cpp:59-171) */
+static int g_density_fix = 0; /* farfield_density_fix of the current run */
+
 static void ghost(int type, const double* fs, const double* Vd, const double* S, double* Vg) {
   double n[3];
   normalize(S, n, NULL);
@@ -106,7 +108,8 @@ static void ghost(int type, const double* fs, const double* Vd, const double* S,
       for (int d = 0; d < 3; d++) Vg[d + 1] = fs[d + 1] + (vn_fs - vn_b) * n[d];
       s_b = s_fs;
     }
-    const double rho_b = pow(GAMMA * s_b / (c_b * c_b), G1_INV);
+    const double rho_b = g_density_fix ? pow(c_b * c_b / (GAMMA * s_b), G1_INV)
+                                       : pow(GAMMA * s_b / (c_b * c_b), G1_INV);
     Vg[0] = rho_b;
     Vg[4] = c_b * c_b * rho_b / GAMMA;
   } else { /* BC_NoSlipWall */
@@ -263,6 +266,7 @@ int nfo_run(const nfo_mesh* m, const nfo_params* p, double* U, int64_t n_steps, 
   w.Vmin = (double*)calloc((size_t)(5 * w.NC), sizeof(double));
   w.R = (double*)calloc((size_t)(5 * w.NC), sizeof(double));
   w.face_patch = (int*)calloc((size_t)w.NF, sizeof(int));
+  g_density_fix = p->farfield_density_fix;
   w.ratchet = 0;
   w.Lf = p->limiter_ratchet_step > 0 ? (double*)malloc(sizeof(double) * 5 * w.NC) : NULL;
   if (w.Lf)

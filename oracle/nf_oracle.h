@@ -47,6 +47,8 @@ typedef struct {
   int64_t limiter_ratchet_step; /* extension: > 0 ratchets the Barth limiter from that step on (0-based):
                                    every stage takes the minimum of its live value and the value
                                    it kept, and keeps that; 0 keeps the limiter live */
+  int farfield_density_fix;      /* extension: 1 = isentropic far-field ghost density instead of the
+                                    reference's inverted form (Numerics.cpp:149) */
 } nfo_params;
 
 /* Advance U (AoS [n_cells][5], in/out) by n_steps of calc_timestep + step.
