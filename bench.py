@@ -276,7 +276,7 @@ def main():
     t_mesh = time.perf_counter() - t0
     cfg = S.Config(precision=args.precision, CFL=0.8, local_time_stepping=lts, density_fs=fs[0],
                    velocity_fs=list(fs[1:4]), pressure_fs=fs[4])
-    solver = S.EulerSolver(cfg, mesh, U0=U0, block_size=args.block, variant=args.variant)
+    solver = S.EulerSolver(cfg, mesh, U0=U0, block_size=args.block, variant=args.variant, device=local)
     lib = L.load()
     N = mesh.n_cells
 
@@ -357,7 +357,7 @@ def main():
         scfg = S.Config(precision=args.precision, CFL=0.8, local_time_stepping=True, density_fs=fs[0],
                         velocity_fs=list(fs[1:4]), pressure_fs=fs[4], **lim)
         solver.close()
-        solver = S.EulerSolver(scfg, mesh, U0=U0)
+        solver = S.EulerSolver(scfg, mesh, U0=U0, device=local)
         solver.tune()
         out = solver.solve_steady(tol=1e-6, max_steps=args.steady_max, check_every=100)
         steady = {"tol": 1e-6, "limiter": args.steady_limiter, "converged": bool(out["converged"][0]),

@@ -177,6 +177,7 @@ typedef struct {
    * inverted form (Numerics.cpp:149), which is exact only for a free-stream
    * density of 1. */
   int farfield_density_fix;
+  int device;           /* CUDA device of the solver; -1 (default): the calling thread's current device */
 } nf_params;
 
 void nf_params_default(nf_params* p);

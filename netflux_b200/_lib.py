@@ -57,7 +57,7 @@ class NfParams(C.Structure):
                 ("patches", C.POINTER(NfPatchBC)), ("n_patches", C.c_int),
                 ("freestream", C.c_double * 5), ("block_size", C.c_int), ("kernel_variant", C.c_int),
                 ("limiter_ratchet_step", C.c_int64), ("limiter_ratchet_drop", C.c_double),
-                ("farfield_density_fix", C.c_int)]
+                ("farfield_density_fix", C.c_int), ("device", C.c_int)]
 
 
 class NetFluxError(RuntimeError):

@@ -693,6 +693,7 @@ void nf_params_default(nf_params* p) {
   p->flux_scheme = NF_FLUX_RUSANOV;
   p->precision = NF_PREC_FP64;
   p->cfl = 0.8;
+  p->device = -1;
   p->freestream[0] = 1.225;   // standard air (Utilities.hpp:100-107)
   p->freestream[4] = 101325.0;
 }
@@ -724,6 +725,7 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
       s->tuned = true;  // a caller-fixed shape is not tuned
     }
     if (s->block % 32 || s->block > 256) throw std::runtime_error("block_size must be a multiple of 32, <= 256");
+    if (p.device >= 0) ck(cudaSetDevice(p.device), "cudaSetDevice");
     ck(cudaGetDevice(&s->device), "cudaGetDevice");
     ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     cudaStream_t st = s->stream;

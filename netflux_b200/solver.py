@@ -210,7 +210,7 @@ class Mesh:
 
 def make_params(config: Config, mesh: Mesh, keep_stage_fields: bool = False,
                 patch_states: Optional[Sequence[Sequence[float]]] = None,
-                block_size: int = 0, variant: int = 0) -> "tuple[L.NfParams, object]":
+                block_size: int = 0, variant: int = 0, device: int = -1) -> "tuple[L.NfParams, object]":
     """nf_params for ``config`` on ``mesh`` (the patch array is returned too, to keep it alive)."""
     p = L.NfParams()
     L.load().nf_params_default(C.byref(p))
@@ -228,6 +228,7 @@ def make_params(config: Config, mesh: Mesh, keep_stage_fields: bool = False,
     p.limiter_ratchet_step = config.limiter_ratchet_step
     p.limiter_ratchet_drop = config.limiter_ratchet_drop
     p.farfield_density_fix = int(config.farfield_density_fix)
+    p.device = int(device)
     for k in range(5):
         p.freestream[k] = config.primvars_inf[k]
     arr = None
@@ -273,11 +274,13 @@ class EulerSolver:
     """EulerSolver(config, grid): the device solver for one (possibly batched) mesh."""
 
     def __init__(self, config: Config, mesh: Mesh, U0: Optional[np.ndarray] = None,
-                 keep_stage_fields: bool = False, patch_states=None, block_size: int = 0, variant: int = 0):
+                 keep_stage_fields: bool = False, patch_states=None, block_size: int = 0, variant: int = 0,
+                 device: int = -1):
         self.mesh = mesh
         self.config = config
         self.n_cells = mesh.n_cells
-        params, self._patch_arr = make_params(config, mesh, keep_stage_fields, patch_states, block_size, variant)
+        params, self._patch_arr = make_params(config, mesh, keep_stage_fields, patch_states, block_size, variant,
+                                              device)
         self._h = L.load().nf_create(mesh._h, C.byref(params))
         if not self._h:
             raise L.NetFluxError(L.NF_ERR_ARG, L.last_error(None))

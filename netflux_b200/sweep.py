@@ -1,6 +1,7 @@
 """Batched bump-channel sweep and the surrogate warm-start study.
 
     python -m netflux_b200.sweep --cases 64 --nx 16 40 --eval-pairs 16 --eval-nx 40 --out DIR
+    torchrun --nproc-per-node N -m netflux_b200.sweep ...   (cases sharded over N GPUs)
 
 1. Sweep: `cases` bump channels (seeded hex resolution nx, ny = nz = nx / 2,
    inflow Mach and bump height) are concatenated into one device mesh with
@@ -44,8 +45,41 @@ def case_mesh(c: Dict) -> S.Mesh:
     return S.Mesh.from_tet_mesh(mg.bump_mesh(c["nx"], c["nx"] // 2, c["nx"] // 2, h=c["h"]))
 
 
+def case_work(c: Dict) -> float:
+    """Estimated cost of one case: cells (1.5 nx^3) times steps to converge (about nx^1.6)."""
+    return 1.5 * c["nx"] ** 3 * c["nx"] ** 1.6
+
+
+def partition_cases(cases: List[Dict], world: int) -> List[List[int]]:
+    """Whole cases per rank, longest first onto the least-loaded rank."""
+    order = sorted(range(len(cases)), key=lambda i: -case_work(cases[i]))
+    load = [0.0] * world
+    parts: List[List[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = int(np.argmin(load))
+        parts[r].append(i)
+        load[r] += case_work(cases[i])
+    return [sorted(p) for p in parts]
+
+
+def run_sharded(cases: List[Dict], rank: int, world: int, gather, run=None, **kw):
+    """This rank's share of the cases as one batched solve; the per-case records
+    of every rank gathered (gather: list of this rank's items -> list over ranks).
+    There is no collective on the data path: cases are independent."""
+    run = run or run_batched
+    parts = partition_cases(cases, world)
+    mine = [cases[i] for i in parts[rank]]
+    res = run(mine, **kw) if mine else {"per_case": []}
+    gathered = gather(list(zip(parts[rank], res["per_case"])))
+    merged = [None] * len(cases)
+    for recs in gathered:
+        for i, r in recs:
+            merged[i] = r
+    return merged, res, parts[rank]
+
+
 def run_batched(cases: List[Dict], precision: str = "mixed", tol: float = 1e-6, max_steps: int = 400000,
-                check_every: int = 100) -> Dict:
+                check_every: int = 100, device: int = -1) -> Dict:
     t0 = time.perf_counter()
     meshes = [case_mesh(c) for c in cases]
     fss = [mg.bump_freestream(c["mach"]) for c in cases]
@@ -53,7 +87,7 @@ def run_batched(cases: List[Dict], precision: str = "mixed", tol: float = 1e-6, 
     t_mesh = time.perf_counter() - t0
     states = [list(fs) for fs, m in zip(fss, meshes) for _ in m.patches()]
     U0 = np.concatenate([mg.uniform_state(m.n_cells, fs) for fs, m in zip(fss, meshes)])
-    s = S.EulerSolver(sur.steady_config(fss[0], precision), batch, U0=U0, patch_states=states)
+    s = S.EulerSolver(sur.steady_config(fss[0], precision), batch, U0=U0, patch_states=states, device=device)
     s.tune()
     out = s.solve_steady(tol, max_steps, check_every)
     U = s.get_solver_data().get_solution()
@@ -125,15 +159,48 @@ def main(argv=None):
     summary = {"args": vars(a)}
 
     cases = sample_cases(a.cases, a.seed, a.nx[0], a.nx[1], a.mach, a.h)
-    res = run_batched(cases, a.precision, a.tol, a.max_steps)
-    summary["sweep"] = {k: v for k, v in res.items() if k not in ("U", "meshes", "offsets")}
-    print(json.dumps({"sweep_cells": res["cells"], "total_ms": res["total_ms"],
-                      "mcell_stages_per_s": res["mcell_stages_per_s"],
-                      "converged": sum(c["converged"] for c in res["per_case"])}), flush=True)
-    F, T = training_data(res, cases)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        # one process per GPU; cases are sharded whole, the only exchange is
+        # the final gather of records and training arrays (gloo, host side)
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=3600))
+
+        def gather(items):
+            out = [None] * world
+            dist.all_gather_object(out, items)
+            return out
+        local = int(os.environ.get("LOCAL_RANK", rank))
+        merged, res, mine = run_sharded(cases, rank, world, gather, precision=a.precision, tol=a.tol,
+                                        max_steps=a.max_steps, device=local)
+        sub = [cases[i] for i in mine]
+        FT = training_data(res, sub) if sub else (np.zeros((0, 7), np.float32), np.zeros((0, 5), np.float32))
+        parts = gather([FT])
+        times = gather([res.get("total_ms", 0.0)])
+        if rank != 0:
+            dist.barrier()
+            dist.destroy_process_group()
+            return
+        F = np.concatenate([p[0][0] for p in parts])
+        T = np.concatenate([p[0][1] for p in parts])
+        work = sum(3.0 * r["cells"] * r["steps"] for r in merged)
+        total_ms = max(t[0] for t in times)
+        summary["sweep"] = {"per_case": merged, "cells": int(sum(r["cells"] for r in merged)), "ranks": world,
+                            "total_ms": total_ms, "mcell_stages_per_s": work / (total_ms * 1e-3) / 1e6}
+    else:
+        res = run_batched(cases, a.precision, a.tol, a.max_steps)
+        summary["sweep"] = {k: v for k, v in res.items() if k not in ("U", "meshes", "offsets")}
+        F, T = training_data(res, cases)
+        del res
+    sw = summary["sweep"]
+    print(json.dumps({"sweep_cells": sw["cells"], "total_ms": sw["total_ms"],
+                      "mcell_stages_per_s": sw["mcell_stages_per_s"],
+                      "converged": sum(c["converged"] for c in sw["per_case"])}), flush=True)
     if a.save_data:
         np.savez_compressed(a.save_data, features=F, targets=T, cases=json.dumps(cases))
-    del res
 
     mlp = sur.MLP(seed=a.seed)
     mlp.set_data(F, T)
@@ -157,6 +224,10 @@ def main(argv=None):
     with open(os.path.join(a.out, "summary.json"), "w") as f:
         json.dump(summary, f, indent=1, default=float)
     print(json.dumps(summary["eval_summary"]), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":
