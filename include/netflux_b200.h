@@ -187,6 +187,14 @@ nf_solver* nf_create(const nf_mesh* m, const nf_params* params);
  * the primitives the next nf_calc_timestep reads. */
 int nf_set_state(nf_solver* s, const double* U, int64_t n_cells);
 int nf_get_state(nf_solver* s, double* U, int64_t n_cells);
+/* U^n of the next step's TVD-RK3 combination (the reference's solution_old,
+ * Solver.cpp:127-132), AoS [n_cells][5] in reference cell order; applies to
+ * the next step only (afterwards U^n is the state, Solver.cpp:51).
+ * nf_set_state makes U^n the state itself. NetFlux's own free-stream start
+ * writes only solution (set_freestream_values, SolverData.cpp:50-58), so its
+ * first RK3 step combines with a zero solution_old; the drop-in passes that
+ * array through here to reproduce the reference program exactly. */
+int nf_set_state_old(nf_solver* s, const double* U_old, int64_t n_cells);
 /* Global dt = min_i CFL*vol_i/sum_d (|u_d|+c) dS_i,d (or the per-cell dt
  * with local time stepping, then *dt_out is its minimum). */
 int nf_calc_timestep(nf_solver* s, double* dt_out);

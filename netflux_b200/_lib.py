@@ -28,7 +28,7 @@ NF_PREC_FP64_REF, NF_PREC_FP64, NF_PREC_MIXED = 0, 1, 2
 EXPORTED = (
     "nf_mesh_from_su2", "nf_mesh_from_arrays", "nf_mesh_concat", "nf_mesh_get_info", "nf_mesh_get_patch",
     "nf_mesh_export", "nf_mesh_get_permutation", "nf_mesh_get_case_offsets", "nf_mesh_destroy",
-    "nf_params_default", "nf_create", "nf_set_state", "nf_get_state", "nf_calc_timestep", "nf_set_timestep",
+    "nf_params_default", "nf_create", "nf_set_state", "nf_get_state", "nf_set_state_old", "nf_calc_timestep", "nf_set_timestep",
     "nf_step", "nf_advance", "nf_get_residual", "nf_get_field", "nf_synchronize", "nf_last_error", "nf_destroy",
     "nf_time_steps", "nf_residual_norms_noalloc", "nf_tune", "nf_solve_steady", "nf_solve_steady_to",
     "nf_mlp_param_count", "nf_mlp_create", "nf_mlp_last_error", "nf_mlp_destroy", "nf_mlp_get_params",
@@ -94,6 +94,7 @@ def load() -> C.CDLL:
         "nf_create": (P, [P, C.POINTER(NfParams)]),
         "nf_set_state": (I, [P, dp, I64]),
         "nf_get_state": (I, [P, dp, I64]),
+        "nf_set_state_old": (I, [P, dp, I64]),
         "nf_calc_timestep": (I, [P, dp]),
         "nf_set_timestep": (I, [P, D]),
         "nf_step": (I, [P]),

@@ -169,6 +169,8 @@ struct nf_solver {
   DevBuf<nf::PatchBC> patches;
   // state
   DevBuf<double> U, W, V0, V1, fs, grad, phi, R, dt_local, res_cell, scal, part, res_out, vg, fb;
+  DevBuf<double> Uold;       // U^n of the next step when set apart from U (nf_set_state_old)
+  bool old_pending = false;
   DevBuf<float> fs32, grad32, phi32, fb32;  // mixed: increments, fields, boundary flux differences
   DevBuf<unsigned> status;
   DevBuf<long long> chunk_begin, chunk_end, case_cells;
@@ -295,6 +297,13 @@ struct nf_solver {
   // n x (calc_timestep + step), replays of a two-step CUDA graph where
   // possible; the ratchet starts at its step.
   void run_steps(int64_t n) {
+    if (n > 0 && old_pending) {  // this step's U^n is not U: outside the graphs
+      ratchet_due(1);
+      enqueue_dt();
+      enqueue_step();
+      steps_done++;
+      n--;
+    }
     while (n > 0) {
       int64_t left = ratchet_due(n);
       n -= left;
@@ -462,11 +471,11 @@ struct nf_solver {
         a.Uout = W.p;
       } else if (s == 1) {
         a.Uin = W.p;
-        a.Un = U.p;
+        a.Un = old_pending ? Uold.p : U.p;
         a.Uout = W.p;
       } else {
         a.Uin = W.p;
-        a.Un = U.p;
+        a.Un = old_pending ? Uold.p : U.p;
         a.Uout = U.p;
       }
       if (p.precision == NF_PREC_MIXED) {
@@ -497,6 +506,7 @@ struct nf_solver {
     scal_kernel<<<1, 1, 0, stream>>>(scal.p, 1, status.p);
     prof_end();
     stepped = true;
+    old_pending = false;  // solution_old = solution (Solver.cpp:51)
   }
 
   // Report a device-side failure as the reference would have (exceptions in
@@ -1060,11 +1070,30 @@ int nf_set_state(nf_solver* s, const double* U, int64_t n_cells) {
     }
     s->vcur = 0;
     s->stepped = false;
+    s->old_pending = false;
     s->steps_done = 0;
     s->ratchet_reset();
     ck(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream), "status reset");
     ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
     ck(cudaGetLastError(), "nf_set_state");
+    return NF_OK;
+  });
+}
+
+int nf_set_state_old(nf_solver* s, const double* U_old, int64_t n_cells) {
+  return guarded(s, [&]() -> int {
+    if (!U_old || n_cells != s->n) {
+      s->err = "nf_set_state_old: state size does not match the mesh";
+      return NF_ERR_ARG;
+    }
+    if (!s->Uold.p) s->Uold.alloc(size_t(5) * s->stride);
+    ck(cudaMemcpyAsync(s->stage.p, U_old, size_t(5) * s->n * sizeof(double), cudaMemcpyHostToDevice, s->stream),
+       "U_old H2D");
+    scatter_state_kernel<<<(s->n + 255) / 256, 256, 0, s->stream>>>(s->n, s->stride, s->d_dev_of_ref.p, s->stage.p,
+                                                                   s->Uold.p);
+    ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
+    ck(cudaGetLastError(), "nf_set_state_old");
+    s->old_pending = true;
     return NF_OK;
   });
 }

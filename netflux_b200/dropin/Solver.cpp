@@ -11,9 +11,10 @@
 // side table keyed by the object's address.
 //
 // Mapping (reference -> here):
-//   EulerSolver ctor (Solver.cpp:135-142)   device mesh from the PrimalGrid
-//                                           arrays, nf_create, nf_set_state
-//                                           with the free-stream solution
+//   EulerSolver ctor (Solver.cpp:135-142)   device mesh from the PrimalGrid /
+//                                           FV_Grid arrays, nf_create,
+//                                           nf_set_state with the solution and
+//                                           nf_set_state_old with solution_old
 //                                           (SolverData.cpp:50-58)
 //   EulerSolver::calc_timestep (232-274)    nf_calc_timestep; the reference's
 //                                           "Invalid dt calculated" throw
@@ -38,17 +39,20 @@ using namespace geometry;
 
 namespace {
 
+// Never destroyed, so the exit handler below can still walk it.
 std::map<const Solver*, nf_solver*>& table() {
-  static std::map<const Solver*, nf_solver*> t;
-  return t;
+  static auto* t = new std::map<const Solver*, nf_solver*>;
+  return *t;
 }
 
-struct Cleanup {
-  ~Cleanup() {
-    for (auto& kv : table()) nf_destroy(kv.second);
-    table().clear();
-  }
-} g_cleanup;
+// Device solvers are released at exit by a handler registered after the
+// first one is created: handlers run in reverse order of registration, so
+// this one runs before the CUDA runtime's own teardown (a static object's
+// destructor could run after it).
+void release_all() {
+  for (auto& kv : table()) nf_destroy(kv.second);
+  table().clear();
+}
 
 nf_solver* device_of(const Solver* s) {
   auto it = table().find(s);
@@ -77,11 +81,15 @@ int precision_from_env() {
   throw std::runtime_error(std::string("NETFLUX_B200_PRECISION: unknown value ") + v);
 }
 
-// The device mesh from the grid PrimalGrid read (PrimalGrid.cpp:140-244).
+// The device mesh from the grids Driver built: nodes and tetrahedra from
+// PrimalGrid (PrimalGrid.cpp:140-244), the boundary from FV_Grid, which has
+// consumed PrimalGrid's element patches by then (FV_Grid.cpp:142) and keeps
+// every face's nodes in face order (face_elements, reordered with the faces,
+// FV_Grid.cpp:207-226): patch q is faces [FIRST_FACE, FIRST_FACE + N_FACES).
 // nf_mesh_from_arrays takes tets in the order an SU2 file lists them and
 // applies the reader's node 1 <-> 2 swap itself (GeometryUtilities.cpp:
 // 452-455), so the swap is undone here.
-nf_mesh* mesh_from_primal(const Config& config, const PrimalGrid& pg) {
+nf_mesh* mesh_from_grids(const PrimalGrid& pg, const FV_Grid& fv) {
   const auto& nodes = pg.get_nodes();
   std::vector<double> xyz(nodes.size() * 3);
   for (size_t i = 0; i < nodes.size(); i++) {
@@ -100,24 +108,27 @@ nf_mesh* mesh_from_primal(const Config& config, const PrimalGrid& pg) {
     tets[4 * size_t(e) + 2] = n[1];
     tets[4 * size_t(e) + 3] = n[3];
   }
-  const auto& patches = pg.get_element_patches();
-  std::vector<const char*> names;
+  const Elements& faces = pg.get_face_elements();
+  std::vector<std::string> names;
   std::vector<int> types;
   std::vector<int64_t> offsets{0}, tris;
-  for (const auto& p : patches) {
-    names.push_back(p.patch_name.c_str());
-    types.push_back(bc_code(config.get_boundary_type(p.patch_name)));
-    const Elements& be = p.boundary_elements;
-    for (Index e = 0; e < be.size(); e++) {
-      const Index* n = be.get_element_nodes(e);
+  for (const auto& p : fv.get_patches()) {
+    names.push_back("patch" + std::to_string(names.size()));
+    types.push_back(bc_code(p.boundary_type));
+    for (Index f = p.FIRST_FACE; f < p.FIRST_FACE + p.N_FACES; f++) {
+      if (faces.get_element_type(f) != ElementType::Triangle)
+        throw std::runtime_error("netflux_b200 supports triangular boundary faces only");
+      const Index* n = faces.get_element_nodes(f);
       tris.push_back(n[0]);
       tris.push_back(n[1]);
       tris.push_back(n[2]);
     }
     offsets.push_back(int64_t(tris.size() / 3));
   }
+  std::vector<const char*> cnames;
+  for (const auto& n : names) cnames.push_back(n.c_str());
   nf_mesh* m = nf_mesh_from_arrays(int64_t(nodes.size()), xyz.data(), int64_t(vol.size()), tets.data(),
-                                   int(names.size()), names.data(), types.data(), offsets.data(), tris.data());
+                                   int(cnames.size()), cnames.data(), types.data(), offsets.data(), tris.data());
   if (!m) throw std::runtime_error(std::string("netflux_b200: ") + nf_last_error(nullptr));
   return m;
 }
@@ -143,7 +154,7 @@ EulerSolver::EulerSolver(const Config& config, const PrimalGrid& primal_grid, co
     : Solver(config, primal_grid, FV_grid) {
   solver_data = make_unique<EulerSolverData>(config);
   validity_checker = make_unique<EulerValidityChecker>(config);
-  nf_mesh* m = mesh_from_primal(config, primal_grid);
+  nf_mesh* m = mesh_from_grids(primal_grid, FV_grid);
   nf_params p;
   nf_params_default(&p);
   p.time_scheme = config.get_time_scheme() == TimeScheme::TVD_RK3 ? NF_TVD_RK3 : NF_EXPLICIT_EULER;
@@ -155,9 +166,15 @@ EulerSolver::EulerSolver(const Config& config, const PrimalGrid& primal_grid, co
   nf_solver* s = nf_create(m, &p);
   nf_mesh_destroy(m);
   if (!s) throw std::runtime_error(std::string("netflux_b200: ") + nf_last_error(nullptr));
+  static const bool registered = (std::atexit(release_all) == 0);
+  (void)registered;
   table()[this] = s;
   const VecField& U = solver_data->get_solution();  // free stream (SolverData.cpp:50-58)
   check(nf_set_state(s, U[0], int64_t(U.size())), s);
+  // solution_old as the reference leaves it (zero after the free-stream
+  // start): the first TVD_RK3 step combines with it (Solver.cpp:127-132)
+  const VecField& U_old = solver_data->get_solution_old();
+  check(nf_set_state_old(s, U_old[0], int64_t(U_old.size())), s);
 }
 
 void EulerSolver::calc_timestep(Config& config) {

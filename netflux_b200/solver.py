@@ -296,6 +296,13 @@ class EulerSolver:
             raise ValueError("state must have shape (n_cells, 5)")
         _check(L.load().nf_set_state(self._h, L.dptr(U), self.n_cells), self._h)
 
+    def set_state_old(self, U_old: np.ndarray) -> None:
+        """U^n of the next RK3 step (the reference's solution_old); see nf_set_state_old."""
+        U_old = np.ascontiguousarray(U_old, dtype=np.float64)
+        if U_old.shape != (self.n_cells, 5):
+            raise ValueError("state must have shape (n_cells, 5)")
+        _check(L.load().nf_set_state_old(self._h, L.dptr(U_old), self.n_cells), self._h)
+
     def calc_timestep(self, config: Config) -> None:
         dt = C.c_double()
         rc = L.load().nf_calc_timestep(self._h, C.byref(dt))

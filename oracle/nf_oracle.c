@@ -285,7 +285,7 @@ int nfo_run(const nfo_mesh* m, const nfo_params* p, double* U, int64_t n_steps, 
   for (int q = 0; q < m->n_patches; q++)
     for (int64_t f = m->patch_first[q]; f < m->patch_first[q] + m->patch_n[q]; f++) w.face_patch[f] = q;
   for (int64_t i = 0; i < w.NC; i++) cons_to_prim(U + 5 * i, w.V + 5 * i);
-  memcpy(Un, U, sizeof(double) * 5 * w.NC);
+  memcpy(Un, p->U_old_first ? p->U_old_first : U, sizeof(double) * 5 * w.NC);
   for (int64_t n = 0; n < n_steps; n++) {
     /* Driver::solve: calc_timestep then step. The primitives are those of the
      * last evaluated stage (Solver.cpp:250) unless the extension asks for

@@ -49,6 +49,9 @@ typedef struct {
                                    it kept, and keeps that; 0 keeps the limiter live */
   int farfield_density_fix;      /* extension: 1 = isentropic far-field ghost density instead of the
                                     reference's inverted form (Numerics.cpp:149) */
+  const double* U_old_first;     /* U^n of the first step's RK3 combination ([n_cells][5]); NULL = the
+                                    initial state. The reference's free-stream start leaves its
+                                    solution_old at zero (SolverData.cpp:50-58, Solver.cpp:127-132) */
 } nfo_params;
 
 /* Advance U (AoS [n_cells][5], in/out) by n_steps of calc_timestep + step.

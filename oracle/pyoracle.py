@@ -35,7 +35,7 @@ class _Params(C.Structure):
     _fields_ = [("time_scheme", C.c_int), ("spatial_order", C.c_int), ("limiter", C.c_int),
                 ("local_time_stepping", C.c_int), ("dt_from_current_state", C.c_int),
                 ("cfl", C.c_double), ("t_end", C.c_double), ("limiter_ratchet_step", C.c_int64),
-                ("farfield_density_fix", C.c_int)]
+                ("farfield_density_fix", C.c_int), ("U_old_first", C.POINTER(C.c_double))]
 
 
 _lib = None
@@ -61,7 +61,8 @@ def run_oracle(grid: Dict[str, np.ndarray], patches: Sequence[dict], patch_fs: S
                U0: np.ndarray, n_steps: int, time_scheme: int = 1, spatial_order: int = 1, limiter: int = 1,
                cfl: float = 0.8, local_time_stepping: bool = False, dt_from_current_state: bool = False,
                t_end: float = 0.0, n_interior_faces: Optional[int] = None, fields: bool = True,
-               limiter_ratchet_step: int = 0, farfield_density_fix: bool = False) -> Dict[str, np.ndarray]:
+               limiter_ratchet_step: int = 0, farfield_density_fix: bool = False,
+               U_old_first: Optional[np.ndarray] = None) -> Dict[str, np.ndarray]:
     """Run the C restatement; ``grid`` is Mesh.export() (reference order).
 
     ``limiter_ratchet_step`` > 0 (extension): from that step on every stage's Barth
@@ -80,8 +81,9 @@ def run_oracle(grid: Dict[str, np.ndarray], patches: Sequence[dict], patch_fs: S
               _dp(keep["rj"]), _dp(keep["vol"]), _dp(keep["dS"]), len(patches),
               ptype.ctypes.data_as(C.POINTER(C.c_int)), pfirst.ctypes.data_as(C.POINTER(C.c_int64)),
               pn.ctypes.data_as(C.POINTER(C.c_int64)), _dp(pfs))
+    U_old = np.ascontiguousarray(U_old_first, np.float64) if U_old_first is not None else None  # kept alive
     p = _Params(time_scheme, spatial_order, limiter, int(local_time_stepping), int(dt_from_current_state), cfl, t_end,
-                int(limiter_ratchet_step), int(farfield_density_fix))
+                int(limiter_ratchet_step), int(farfield_density_fix), _dp(U_old))
     U = np.ascontiguousarray(U0, dtype=np.float64).copy()
     out = {"dt": np.zeros(max(n_steps, 1)), "res": np.zeros((max(n_steps, 1), 2)), "time": np.zeros(1)}
     if fields:

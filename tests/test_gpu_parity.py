@@ -185,6 +185,26 @@ def test_limiter_ratchet_matches_oracle(precision, tol_l2):
     assert rel_l2(live["U"], o["U"]) > 10 * tol_l2
 
 
+@pytest.mark.parametrize("precision,tol", [("fp64_ref", 1e-13), ("fp64", 1e-12)])
+def test_set_state_old_reproduces_the_reference_free_stream_start(precision, tol):
+    """U^n of the first RK3 step set apart from the state (zero, as NetFlux's own free-stream start
+    leaves solution_old), through graph replays and through single steps."""
+    g = golden("bump12")
+    zero = np.zeros_like(g["U0"])
+    o = _oracle(g, 10, U_old_first=zero, fields=False)
+    s, _, _ = run(g, precision, 0)
+    s.set_state_old(zero)
+    s.advance(10)
+    assert rel_linf(s.get_solver_data().get_solution(), o["U"]) <= tol
+    s2, U2, _ = run(g, precision, 0)
+    s2.set_state_old(zero)
+    cfg = s2.config
+    for _ in range(10):
+        s2.calc_timestep(cfg)
+        s2.step(cfg)
+    assert rel_linf(s2.get_solver_data().get_solution(), o["U"]) <= tol
+
+
 def test_t_end_clipping_matches_oracle():
     g = golden("sod40")
     t_end = 0.9 * 5 * float(g["dt1"][0])

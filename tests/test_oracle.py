@@ -116,3 +116,24 @@ def test_reference_with_debug_dump_agrees(tmp_path):
     mg.write_case(str(tmp_path / "case"), m, tuple(g["freestream"]), U0=g["U0"])
     a = po.run_reference(str(tmp_path / "case"), 1, variant="nf_ref")
     assert np.array_equal(a["U"], g["U1"])
+
+
+def test_reference_free_stream_start_leaves_solution_old_zero(tmp_path):
+    """NetFlux's own free-stream start writes only `solution` (SolverData.cpp:50-58), so its first
+    TVD-RK3 step combines with a zero solution_old (Solver.cpp:127-132). The oracle reproduces the
+    reference program bit for bit with U_old_first = 0, and differs from it without."""
+    if not po.reference_available():
+        pytest.skip("compiled reference not built")
+    from netflux_b200 import solver as S
+    m = mg.bump_mesh(8, 4, 4, h=0.1)
+    fs = mg.bump_freestream(0.5)
+    case = str(tmp_path / "case")
+    mg.write_case(case, m, fs)  # no U0.bin: the reference initialises itself
+    ref = po.run_reference(case, 3)
+    mm = S.Mesh.from_tet_mesh(m)
+    pats = mm.patches()
+    U0 = mg.uniform_state(mm.n_cells, fs)
+    o = po.run_oracle(mm.export(), pats, [fs] * len(pats), U0, 3, U_old_first=np.zeros_like(U0), fields=False)
+    assert np.array_equal(o["U"], ref["U"])
+    o2 = po.run_oracle(mm.export(), pats, [fs] * len(pats), U0, 3, fields=False)
+    assert not np.allclose(o2["U"], ref["U"])
