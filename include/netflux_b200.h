@@ -273,6 +273,11 @@ void nf_destroy(nf_solver* s);
 int nf_residual_norms_noalloc(const double* values, int64_t n, double* out, void* stream);
 
 
+/* Self-test of the fast forms' reciprocal and reciprocal square root (a
+ * single-precision estimate refined by two Newton-Raphson steps) on n
+ * positive inputs; no reference counterpart. */
+int nf_fastmath_selftest(const double* x, int64_t n, double* rcp_out, double* rsqrt_out);
+
 /* ------------------------------------------------------------------------
  * Surrogate MLP for warm starts (extension; the reference has no learned
  * part). 7 inputs (cell centroid x, y, z, wall distance, Mach, bump height,

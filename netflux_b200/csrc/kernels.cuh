@@ -465,9 +465,9 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
   if (c >= m.n || frozen_cell(a, c)) return;
   const int st = m.stride;
   static_assert(sizeof(T) == 8, "FP64 kernel");
-  const T* Vin = a.Vin;
-  const T* Vg = a.vg;
-  T* fs = a.fs;
+  const T* __restrict__ Vin = a.Vin;
+  const T* __restrict__ Vg = a.vg;
+  T* __restrict__ fs = a.fs;
   int nb[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) nb[q] = m.nbvf[q * st + c];
@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
   }
   const T ssum[3] = {(S[0][0] + S[1][0]) + (S[2][0] + S[3][0]), (S[0][1] + S[1][1]) + (S[2][1] + S[3][1]),
                      (S[0][2] + S[1][2]) + (S[2][2] + S[3][2])};
-  const T hv = T(0.5 / m.vol[c]);
+  const T hv = T(0.5) * nr_rcp(T(m.vol[c]));
   const bool rat = a.barth && ratchet_on(a, c);
 #pragma unroll 1
   for (int k = 0; k < 5; k++) {
@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
         An = better ? A : An;
         Dn = better ? D : Dn;
       }
-      phi = An / Dn;
+      phi = An * nr_rcp(Dn);
       if (rat) phi = ratchet(a, size_t(k) * st + c, phi);
     }
 #pragma unroll
@@ -570,16 +570,17 @@ struct FaceIn {
 __device__ __forceinline__ void stage_update(const StageArgs& a, int c, int st, const double R[5], double vol) {
   const double dt = a.local_dt ? a.dt_local[c] : stage_dt(a.scal);
   double Unew[5];
+  const double ivol = nr_rcp(vol);
   if (a.scheme == 0 || a.stage == 0) {
-    const double qf = dt / vol;
+    const double qf = dt * ivol;
 #pragma unroll
     for (int k = 0; k < 5; k++) Unew[k] = fma(qf, R[k], a.Uin[k * st + c]);
   } else if (a.stage == 1) {
-    const double qf = 0.25 * dt / vol;
+    const double qf = 0.25 * dt * ivol;
 #pragma unroll
     for (int k = 0; k < 5; k++) Unew[k] = 0.75 * a.Un[k * st + c] + 0.25 * a.Uin[k * st + c] + qf * R[k];
   } else {
-    const double qf = 2.0 / 3.0 * dt / vol;
+    const double qf = 2.0 / 3.0 * dt * ivol;
 #pragma unroll
     for (int k = 0; k < 5; k++) Unew[k] = 1.0 / 3.0 * a.Un[k * st + c] + 2.0 / 3.0 * a.Uin[k * st + c] + qf * R[k];
   }
@@ -597,7 +598,7 @@ __device__ __forceinline__ void stage_update(const StageArgs& a, int c, int st, 
     if (a.R) a.R[k * st + c] = R[k];
     finite = finite && isfinite(R[k]) && isfinite(Unew[k]);
   }
-  if (a.res_cell) a.res_cell[c] = R[0] / vol;
+  if (a.res_cell) a.res_cell[c] = R[0] * ivol;
   if (!finite) atomicOr(a.status, kErrNonFinite);
   else if (!(Vn[0] > 0.0) || !(Vn[4] > 0.0)) atomicOr(a.status, kErrNonPhysical);
 }
@@ -609,9 +610,9 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
   const int st = m.stride;
   const bool second = a.second_order != 0;
   static_assert(sizeof(T) == 8, "FP64 kernel");
-  const T* fsb = a.fs;
-  const T* Vin = a.Vin;
-  const T* fb = a.fb;
+  const T* __restrict__ fsb = a.fs;
+  const T* __restrict__ Vin = a.Vin;
+  const T* __restrict__ fb = a.fb;
   const int code = m.gcode[c];
   int ns[4];
 #pragma unroll
@@ -662,8 +663,8 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
       // owner-to-neighbour normal: this cell's outward normal on the owner side
       const bool flip = own ? (bits & 2) != 0 : (bits & 2) == 0;
       const T a2 = (S[q][0] * S[q][0] + S[q][1] * S[q][1]) + S[q][2] * S[q][2];
-      const T area = sqrt(a2);
-      const T inv = T(1) / area;
+      const T inv = nr_rsqrt(a2);  // 1 / |S|
+      const T area = a2 * inv;
       const T sg = flip ? -inv : inv;
       const T nh[3] = {S[q][0] * sg, S[q][1] * sg, S[q][2] * sg};
       T Fl[5];

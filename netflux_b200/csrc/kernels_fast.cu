@@ -78,6 +78,16 @@ void launch_bflux_fast(const MeshView<double>& m, const StageArgs& a, Launch l) 
 void launch_bflux_mixed(const MeshView<double>& m, const StageArgs& a, Launch l) {
   if (m.nb > 0) boundary_flux_delta_kernel<<<grid_for(m.nb, l.block), l.block, 0, l.stream>>>(m, a);
 }
+__global__ void fastmath_kernel(const double* x, int n, double* rcp, double* rsq) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  rcp[i] = nr_rcp(x[i]);
+  rsq[i] = nr_rsqrt(x[i]);
+}
+void launch_fastmath(const double* x, int n, double* rcp, double* rsq, Launch l) {
+  fastmath_kernel<<<grid_for(n, l.block), l.block, 0, l.stream>>>(x, n, rcp, rsq);
+}
+
 void launch_prim_fast(int n, int stride, const double* U, double* V, float* V32, Launch l) {
   prim_kernel_fast<false><<<grid_for(n, l.block), l.block, 0, l.stream>>>(n, stride, U, V, V32);
 }

@@ -53,7 +53,7 @@ __device__ __forceinline__ DeltaSide delta_side(const float vc[5], float q_c, fl
   const float H = fmaf(p, g1i, fmaf(0.5f * rho, uu, p));  // E + p
   o.dU[4] = dE;
   o.dF[4] = fmaf(dE + d[4], q_c, H * dq);
-  o.s = fabsf(q_c + dq) + sqrtf(Gas<float>::gamma * p / rho);
+  o.s = fabsf(q_c + dq) + sound_speed_fast(rho, p);
   return o;
 }
 
@@ -79,6 +79,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshVie
   const int st = m.stride;
   const double* __restrict__ V = a.Vin;
   const double* __restrict__ Vg = a.vg;
+  float* __restrict__ inc_out = a.fs32;
   int nb[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) nb[q] = m.nbvf[q * st + c];
@@ -158,11 +159,11 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshVie
         An = better ? A : An;
         Dn = better ? D : Dn;
       }
-      phi = An / Dn;
+      phi = An * nr_rcp(Dn);
       if (rat) phi = ratchet(a, size_t(k) * st + c, phi);
     }
 #pragma unroll
-    for (int q = 0; q < 4; q++) a.fs32[(q * 5 + k) * st + c] = phi * gr[q];
+    for (int q = 0; q < 4; q++) inc_out[(q * 5 + k) * st + c] = phi * gr[q];
     if (a.grad32) {
 #pragma unroll
       for (int e = 0; e < 3; e++) a.grad32[(k * 3 + e) * st + c] = g[e];
@@ -181,6 +182,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_delta_kernel(MeshView<fl
   const bool second = a.second_order != 0;
   const double* __restrict__ V = a.Vin;
   const float* __restrict__ inc = a.fs32;
+  const float* __restrict__ fbd = a.fb32;
   const int code = m.gcode[c];
   double vcd[5];
   float vc[5];
@@ -202,7 +204,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_delta_kernel(MeshView<fl
       in.kind = 3;
       const int b = -ns[q] - 1;
 #pragma unroll
-      for (int k = 0; k < 5; k++) in.s[k] = a.fb32[k * m.bstride + b];
+      for (int k = 0; k < 5; k++) in.s[k] = fbd[k * m.bstride + b];
     } else {
       const int o = ns[q] >> 2, q2 = ns[q] & 3;
       in.kind = 1;
@@ -244,8 +246,9 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_delta_kernel(MeshView<fl
     } else if (cur.kind == 1) {
       const int bits = code >> (3 * q);
       const float a2 = fmaf(S[q][2], S[q][2], fmaf(S[q][1], S[q][1], S[q][0] * S[q][0]));
-      const float area = sqrtf(a2);
-      const float sg = (bits & 2) ? -1.f / area : 1.f / area;  // outward unit normal
+      const float inv = nr_rsqrt(a2);  // 1 / |S|
+      const float area = a2 * inv;
+      const float sg = (bits & 2) ? -inv : inv;  // outward unit normal
       const float nh[3] = {S[q][0] * sg, S[q][1] * sg, S[q][2] * sg};
       float Fl[5];
       rusanov_delta(vc, cur.s, cur.x, nh, area, Fl);

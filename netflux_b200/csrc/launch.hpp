@@ -34,5 +34,7 @@ void launch_bflux_fast(const MeshView<double>& m, const StageArgs& a, Launch l);
 // stored as FP32 differences to the owner's physical flux
 void launch_bflux_mixed(const MeshView<double>& m, const StageArgs& a, Launch l);
 void launch_prim_fast(int n, int stride, const double* U, double* V, float* V32, Launch l);
+// the fast forms' reciprocal and reciprocal square root, elementwise (self-test)
+void launch_fastmath(const double* x, int n, double* rcp, double* rsq, Launch l);
 
 }  // namespace nf

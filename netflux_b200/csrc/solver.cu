@@ -1453,6 +1453,25 @@ int nf_tune(nf_solver* s, int* config) {
   });
 }
 
+int nf_fastmath_selftest(const double* x, int64_t n, double* rcp_out, double* rsqrt_out) {
+  if (!x || !rcp_out || !rsqrt_out || n <= 0 || n > (int64_t(1) << 26)) return NF_ERR_ARG;
+  try {
+    DevBuf<double> dx, dr, ds;
+    dx.alloc(size_t(n));
+    dr.alloc(size_t(n));
+    ds.alloc(size_t(n));
+    ck(cudaMemcpy(dx.p, x, size_t(n) * sizeof(double), cudaMemcpyHostToDevice), "H2D");
+    nf::launch_fastmath(dx.p, int(n), dr.p, ds.p, nf::Launch{256, nullptr});
+    ck(cudaGetLastError(), "fastmath launch");
+    ck(cudaMemcpy(rcp_out, dr.p, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+    ck(cudaMemcpy(rsqrt_out, ds.p, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+  } catch (const std::exception& e) {
+    nf::set_last_error_text(e.what());
+    return NF_ERR_CUDA;
+  }
+  return NF_OK;
+}
+
 int nf_synchronize(nf_solver* s) {
   return guarded(s, [&]() -> int { return s->check_status(); });
 }

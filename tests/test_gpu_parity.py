@@ -380,3 +380,18 @@ def test_batched_steady_freezes_converged_cases_exactly():
     for k, (o, U) in enumerate(singles):
         assert out["steps"][k] == o["steps"][0]
         assert np.array_equal(Ub[off[k]:off[k + 1]], U)
+
+
+def test_fast_reciprocal_and_rsqrt_within_two_ulp():
+    """The fast FP64 form's 1/x and 1/sqrt(x) (FP32 estimate + two Newton-Raphson steps) against
+    correctly rounded values, over 12 decades either side of 1."""
+    rng = np.random.default_rng(7)
+    x = 10.0 ** rng.uniform(-12, 12, 200000)
+    r = np.empty_like(x)
+    q = np.empty_like(x)
+    assert L.load().nf_fastmath_selftest(L.dptr(x), x.size, L.dptr(r), L.dptr(q)) == L.NF_OK
+    ulp = lambda v: np.spacing(np.abs(v))
+    e_rcp = np.abs(r - 1.0 / x) / ulp(1.0 / x)
+    e_rsq = np.abs(q - 1.0 / np.sqrt(x)) / ulp(1.0 / np.sqrt(x))
+    print("max ulp: rcp", e_rcp.max(), "rsqrt", e_rsq.max())
+    assert e_rcp.max() <= 2 and e_rsq.max() <= 2
