@@ -180,20 +180,20 @@ def model_bytes_per_cell_stage(n_cells: int, n_faces: int) -> float:
     return step / (3.0 * n_cells)
 
 
-def cpu_reference_baseline(n_steps: int = 3, scale_hex=(64, 32, 32), procs: int = 0):
-    """Time the compiled reference on a bounded sample of the bump workload."""
+def cpu_reference_baseline(n_steps: int = 3, case: str = "bump", scale: int = 2, procs: int = 0):
+    """Time the compiled reference on a bounded sample of a workload: the case's
+    mesh (the bump channel at half resolution by default), n_steps TVD-RK3
+    steps per single-threaded process."""
     from netflux_b200 import meshgen as mg
     from oracle import pyoracle as po  # CPU baseline leg only
     variant = "nf_ref_nodump"
     if not po.reference_available(variant):
         return None
-    nx, ny, nz = scale_hex
-    m = mg.bump_mesh(nx, ny, nz, h=0.1)
-    fs = mg.bump_freestream(0.5)
+    m, fs, U0, _, desc = case_mesh(case, scale)
     nproc = procs or (os.cpu_count() or 1)
     with tempfile.TemporaryDirectory() as tmp:
-        case = os.path.join(tmp, "case")
-        mg.write_case(case, m, fs, U0=mg.uniform_state(m.n_cells, fs))
+        case_dir = os.path.join(tmp, "case")
+        mg.write_case(case_dir, m, fs, U0=U0)
         exe = os.path.join(po.REF_DIR, variant)
 
         def run_many(k):
@@ -202,7 +202,7 @@ def cpu_reference_baseline(n_steps: int = 3, scale_hex=(64, 32, 32), procs: int 
                 od = os.path.join(tmp, f"o{i}")
                 os.makedirs(od, exist_ok=True)
                 outs.append(od)
-                ps.append(subprocess.Popen([exe, case, od, "--steps", str(n_steps), "--quiet"], cwd=tmp,
+                ps.append(subprocess.Popen([exe, case_dir, od, "--steps", str(n_steps), "--quiet"], cwd=tmp,
                                            stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
             for p in ps:
                 p.wait()
@@ -220,7 +220,7 @@ def cpu_reference_baseline(n_steps: int = 3, scale_hex=(64, 32, 32), procs: int 
         "single_core": cs / one / 1e6,
         "all_cores": cs * len(many) / max(many) / 1e6,
         "cores": nproc,
-        "sample": f"bump channel {nx}x{ny}x{nz} hexes ({m.n_cells} tets), {n_steps} TVD-RK3 steps per process, "
+        "sample": f"{desc} (hex counts / {scale}: {m.n_cells} tets), {n_steps} TVD-RK3 steps per process, "
                   f"reference compiled from its sources (debug dump linked out), {nproc} independent "
                   f"single-threaded processes",
     }
@@ -235,14 +235,14 @@ def run_reference_arm(args):
         print(json.dumps({"impl": "reference", "unavailable": "reference build (oracle/_ref) missing"}))
         return
     nproc = os.cpu_count() or 1
-    res = cpu_reference_baseline(n_steps=max(1, args.steps), procs=nproc)
+    scale = args.scale if args.case != "bump" else max(2, args.scale)  # the bump sample: half resolution
+    res = cpu_reference_baseline(n_steps=max(1, args.steps), case=args.case, scale=scale, procs=nproc)
     val = res["all_cores"]
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(val, 3), "unit": "Mcell-stages/s",
         "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "bump channel, TVD-RK3 FP64 (sample of the 3.1M-tet case)",
-                   "sample": res["sample"]},
+        "config": {"workload": f"{args.case}, TVD-RK3 FP64 (bounded sample)", "sample": res["sample"]},
         "cpu_baseline": {"value": round(val, 3), "unit": "Mcell-stages/s", "cores": res["cores"],
                          "kind": "reference", "sample": res["sample"],
                          "single_core": round(res["single_core"], 4)},
@@ -368,7 +368,8 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        res = cpu_reference_baseline()
+        # the same workload: the bump channel at half resolution, the small cases whole
+        res = cpu_reference_baseline(case=args.case, scale=max(2, args.scale) if args.case == "bump" else args.scale)
         if res is not None:
             cpu = {"value": round(res["all_cores"], 4), "unit": "Mcell-stages/s", "cores": res["cores"],
                    "kind": "reference", "sample": res["sample"], "single_core": round(res["single_core"], 4)}

@@ -232,9 +232,11 @@ int nf_get_field(nf_solver* s, int which, double* out, int64_t n_values);
 int nf_synchronize(nf_solver* s);
 
 /* Time the launch shapes of the gradient and flux kernels on the current
- * state and keep the fastest: block size (64 or 128 threads) and whether each
+ * state and keep the fastest: block size (64 or 128 threads), whether each
  * thread issues its next variable's / face's loads before the current
- * arithmetic. config (may be NULL) receives {gradient block, gradient
+ * arithmetic (variants 1, 3, 5), and a register cap for occupancy (none,
+ * variants 0-1; 6 / 8 resident 128-thread blocks for FP64 / FP32, variants
+ * 2-3; 7 / 9, variants 4-5). config (may be NULL) receives {gradient block, gradient
  * variant, flux block, flux variant}. The state is unchanged. The reference
  * has no counterpart (it runs on one CPU thread). */
 int nf_tune(nf_solver* s, int* config);
@@ -307,6 +309,9 @@ int nf_mlp_gradients(nf_mlp* m, const float* features, const float* targets, int
                      double* loss_out);
 /* Forward pass: out [n][5]; *ms_out the device time of the kernel. */
 int nf_mlp_predict(nf_mlp* m, const float* features, int64_t n, float* out, double* ms_out);
+/* Distance from each of n points [n][3] to the nearest of m wall points
+ * [m][3] (the surrogate's wall-distance input), out [n]; FP32. */
+int nf_wall_distance(const float* points, int64_t n, const float* wall, int64_t m, float* out);
 /* D[128][N] = A[128][K] B[N][K]^T through the library's tcgen05 path
  * (A, B as BF16 bit patterns, row-major); 16 <= N, K <= 256, multiples of 16. */
 int nf_mlp_gemm_selftest(const uint16_t* A, const uint16_t* B, int N, int K, float* D);

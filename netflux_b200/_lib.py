@@ -33,7 +33,7 @@ EXPORTED = (
     "nf_time_steps", "nf_residual_norms_noalloc", "nf_tune", "nf_solve_steady", "nf_solve_steady_to", "nf_fastmath_selftest",
     "nf_mlp_param_count", "nf_mlp_create", "nf_mlp_last_error", "nf_mlp_destroy", "nf_mlp_get_params",
     "nf_mlp_set_params", "nf_mlp_set_data", "nf_mlp_train", "nf_mlp_gradients", "nf_mlp_predict",
-    "nf_mlp_gemm_selftest",
+    "nf_mlp_gemm_selftest", "nf_wall_distance",
 )
 NF_KERNEL_TIMESTEP, NF_KERNEL_GRADIENT, NF_KERNEL_FLUX, NF_KERNEL_OTHER, NF_KERNEL_COUNT = range(5)
 
@@ -122,6 +122,7 @@ def load() -> C.CDLL:
         "nf_mlp_gradients": (I, [P, fp, fp, I64, fp, dp]),
         "nf_mlp_predict": (I, [P, fp, I64, fp, dp]),
         "nf_mlp_gemm_selftest": (I, [C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), I, I, fp]),
+        "nf_wall_distance": (I, [fp, I64, fp, I64, fp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

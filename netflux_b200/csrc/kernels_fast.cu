@@ -29,9 +29,13 @@ static inline int fast_block(int b) { return b > 128 ? 128 : b; }
 
 // Variants (the tuner times them): 0 plain, 1 software-pipelined, 2 plain
 // with registers capped for at least kCap resident 128-thread blocks per SM
-// (6 for FP64, 8 for FP32), 3 pipelined with the same cap.
+// (6 for FP64, 8 for FP32), 3 pipelined with the same cap, 4 and 5 the same
+// with a tighter cap (7 / 9 blocks).
 template <typename T>
 constexpr int kCap = sizeof(T) == 8 ? 6 : 8;
+// 4 plain, 5 pipelined, registers capped tighter: at least kCap2 blocks
+template <typename T>
+constexpr int kCap2 = sizeof(T) == 8 ? 7 : 9;
 #define NF_NODE_DISPATCH(KERNEL, T, m, a, l)                                                       \
   do {                                                                                              \
     const int b = fast_block(l.block);                                                             \
@@ -40,6 +44,8 @@ constexpr int kCap = sizeof(T) == 8 ? 6 : 8;
       case 1: KERNEL<T, true, 1><<<g, b, 0, l.stream>>>(m, a); break;                             \
       case 2: KERNEL<T, false, kCap<T>><<<g, b, 0, l.stream>>>(m, a); break;                          \
       case 3: KERNEL<T, true, kCap<T>><<<g, b, 0, l.stream>>>(m, a); break;                           \
+      case 4: KERNEL<T, false, kCap2<T>><<<g, b, 0, l.stream>>>(m, a); break;                         \
+      case 5: KERNEL<T, true, kCap2<T>><<<g, b, 0, l.stream>>>(m, a); break;                          \
       default: KERNEL<T, false, 1><<<g, b, 0, l.stream>>>(m, a); break;                           \
     }                                                                                               \
   } while (0)
@@ -59,6 +65,8 @@ void launch_flux_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
       case 1: KERNEL<true, 1><<<g, b, 0, l.stream>>>(m, a); break;                                 \
       case 2: KERNEL<false, kCap<float>><<<g, b, 0, l.stream>>>(m, a); break;                      \
       case 3: KERNEL<true, kCap<float>><<<g, b, 0, l.stream>>>(m, a); break;                       \
+      case 4: KERNEL<false, kCap2<float>><<<g, b, 0, l.stream>>>(m, a); break;                     \
+      case 5: KERNEL<true, kCap2<float>><<<g, b, 0, l.stream>>>(m, a); break;                      \
       default: KERNEL<false, 1><<<g, b, 0, l.stream>>>(m, a); break;                               \
     }                                                                                               \
   } while (0)

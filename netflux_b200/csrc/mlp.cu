@@ -635,6 +635,31 @@ __global__ void __launch_bounds__(128, 1) umma_gemm_test_kernel(const __nv_bfloa
   teardown(tbase, 256);
 }
 
+// Distance from each point to the nearest of m wall points (the surrogate's
+// wall-distance input): one thread per point, wall points staged through
+// shared memory in tiles of 1024.
+constexpr int WD_TILE = 1024;
+__global__ void __launch_bounds__(256) wall_distance_kernel(const float* __restrict__ pts, int64_t n,
+                                                             const float* __restrict__ wall, int64_t m,
+                                                             float* __restrict__ out) {
+  __shared__ float sw[3 * WD_TILE];
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const float px = i < n ? pts[3 * i] : 0.f, py = i < n ? pts[3 * i + 1] : 0.f, pz = i < n ? pts[3 * i + 2] : 0.f;
+  float best = 3.0e38f;
+  for (int64_t t0 = 0; t0 < m; t0 += WD_TILE) {
+    const int cnt = int(m - t0 < WD_TILE ? m - t0 : WD_TILE);
+    __syncthreads();
+    for (int j = threadIdx.x; j < 3 * cnt; j += blockDim.x) sw[j] = wall[3 * t0 + j];
+    __syncthreads();
+#pragma unroll 4
+    for (int j = 0; j < cnt; j++) {
+      const float dx = px - sw[3 * j], dy = py - sw[3 * j + 1], dz = pz - sw[3 * j + 2];
+      best = fminf(best, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+    }
+  }
+  if (i < n) out[i] = sqrtf(best);
+}
+
 }  // namespace mlp
 }  // namespace nf
 
@@ -975,6 +1000,25 @@ int nf_mlp_predict(nf_mlp* m, const float* features, int64_t n, float* out, doub
     m->check_status();
     return NF_OK;
   });
+}
+
+int nf_wall_distance(const float* points, int64_t n, const float* wall, int64_t m, float* out) {
+  if (!points || !wall || !out || n <= 0 || m <= 0) return NF_ERR_ARG;
+  try {
+    Buf<float> p, w, o;
+    p.alloc(size_t(3) * n);
+    w.alloc(size_t(3) * m);
+    o.alloc(size_t(n));
+    ck(cudaMemcpy(p.p, points, size_t(3) * n * sizeof(float), cudaMemcpyHostToDevice), "H2D");
+    ck(cudaMemcpy(w.p, wall, size_t(3) * m * sizeof(float), cudaMemcpyHostToDevice), "H2D");
+    wall_distance_kernel<<<unsigned((n + 255) / 256), 256>>>(p.p, n, w.p, m, o.p);
+    ck(cudaGetLastError(), "wall distance launch");
+    ck(cudaMemcpy(out, o.p, size_t(n) * sizeof(float), cudaMemcpyDeviceToHost), "D2H");
+  } catch (const std::exception& e) {
+    g_mlp_error = e.what();
+    return NF_ERR_CUDA;
+  }
+  return NF_OK;
 }
 
 int nf_mlp_gemm_selftest(const uint16_t* A, const uint16_t* B, int N, int K, float* D) {

@@ -109,8 +109,8 @@ def gemm_selftest(A: np.ndarray, B: np.ndarray) -> np.ndarray:
 # features and targets
 # ---------------------------------------------------------------------------
 def wall_distance(mesh: S.Mesh, grid: Optional[Dict[str, np.ndarray]] = None) -> np.ndarray:
-    """Distance of every cell centroid to the nearest wall-face centroid (slip and no-slip patches)."""
-    from scipy.spatial import cKDTree
+    """Distance of every cell centroid to the nearest wall-face centroid (slip and no-slip patches),
+    on the GPU (nf_wall_distance)."""
     g = grid if grid is not None else mesh.export()
     N = mesh.n_cells
     pts = []
@@ -121,8 +121,11 @@ def wall_distance(mesh: S.Mesh, grid: Optional[Dict[str, np.ndarray]] = None) ->
             pts.append(g["centroid"][i] + g["ri"][f])
     if not pts:
         return np.full(N, FEATURE_HI[3])
-    d, _ = cKDTree(np.concatenate(pts)).query(g["centroid"][:N])
-    return d
+    cen = np.ascontiguousarray(g["centroid"][:N], np.float32)
+    wall = np.ascontiguousarray(np.concatenate(pts), np.float32)
+    out = np.empty(N, np.float32)
+    _check(L.load().nf_wall_distance(L.fptr(cen), N, L.fptr(wall), wall.shape[0], L.fptr(out)), None)
+    return out.astype(np.float64)
 
 
 def features(centroids: np.ndarray, wall_dist: np.ndarray, mach: float, h: float) -> np.ndarray:

@@ -130,6 +130,23 @@ def test_tuning_changes_nothing(precision):
     assert np.array_equal(a.get_solver_data().get_solution(), b.get_solver_data().get_solution())
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_every_launch_variant_computes_the_same_bits(precision):
+    """Every block size and variant the tuner may pick (pipelined loads, register caps) gives the same state."""
+    g = golden("bump12")
+    cfg = config_for(precision=precision, freestream=tuple(g["freestream"]))
+    out = {}
+    for block in (64, 128):
+        for variant in range(6):
+            s = S.EulerSolver(cfg, mesh(g), U0=g["U0"], block_size=block, variant=variant)
+            s.advance(3)
+            out[(block, variant)] = s.get_solver_data().get_solution()
+            s.close()
+    ref = out[(128, 0)]
+    for k, U in out.items():
+        assert np.array_equal(U, ref), k
+
+
 def test_deterministic_repeat():
     g = golden("sod40")
     _, a, _ = run(g, "fp64", 20, use_advance=True)

@@ -101,3 +101,14 @@ def test_warm_start_gains_over_free_stream_start():
     assert warm["res_final"] <= 1e-6 * plain["res_fs"]
     assert warm["steps"] < plain["steps"]
     assert d <= 1e-5
+
+
+def test_wall_distance_matches_brute_force():
+    from netflux_b200 import _lib as L
+    rng = np.random.default_rng(3)
+    pts = rng.uniform(0, 3, (5000, 3)).astype(np.float32)
+    wall = rng.uniform(0, 3, (3001, 3)).astype(np.float32)
+    out = np.empty(5000, np.float32)
+    assert L.load().nf_wall_distance(L.fptr(pts), 5000, L.fptr(wall), 3001, L.fptr(out)) == L.NF_OK
+    ref = np.sqrt(((pts[:, None, :].astype(np.float64) - wall[None, :, :]) ** 2).sum(-1).min(1))
+    assert np.max(np.abs(out - ref)) <= 1e-5 * np.max(ref)
