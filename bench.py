@@ -172,6 +172,15 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
     return {"flux": flux, "gradient": grad}
 
 
+# DRAM bytes per cell of one launch (dram__bytes_read.sum + dram__bytes_write.sum), captured
+# with ncu on the full 3,145,728-tet bump channel (profiles/dram_traffic_bump3M.md); the bump
+# workload's `roofline.traffic` is this times its cells, other workloads report null.
+MEASURED_DRAM_BYTES_PER_CELL = {
+    ("fp64", "gradient"): 775.1e6 / 3145728, ("fp64", "flux"): 1086.5e6 / 3145728,
+    ("mixed", "gradient"): 507.9e6 / 3145728, ("mixed", "flux"): 965.7e6 / 3145728,
+}
+
+
 def model_bytes_per_cell_stage(n_cells: int, n_faces: int) -> float:
     """The per-cell-stage byte model of the step's compulsory traffic (FP64):
     N_c*[3*(40 U read + 40 U write + 8 vol + 240 limited-gradient write+read)
@@ -315,8 +324,10 @@ def main():
     hbm, hbm_kind = measured_peaks()
     dom = max(("flux", "gradient"), key=lambda k: kern[k][0] * kern[k][1])
     ach = ab[dom] / (kern[dom][0] * 1e-3) / 1e9
+    per_cell = MEASURED_DRAM_BYTES_PER_CELL.get((args.precision, dom)) if args.case == "bump" else None
+    traffic = int(per_cell * N) if per_cell else None
     roof = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-            "frac": round(ach / hbm, 4), "peak_kind": hbm_kind, "traffic": None,
+            "frac": round(ach / hbm, 4), "peak_kind": hbm_kind, "traffic": traffic,
             "algorithmic_bytes_per_launch": int(ab[dom]), "avg_launch_ms": round(kern[dom][0], 5),
             "per_kernel_ms": {k: round(v[0], 5) for k, v in kern.items()}}
     model = model_bytes_per_cell_stage(N, mesh.n_faces)
