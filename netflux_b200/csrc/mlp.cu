@@ -351,25 +351,36 @@ __global__ void __launch_bounds__(128, 1) mlp_backward_kernel(BwdArgs a) {
         }
         umma::commit(sync.mbar);
       }
-      if (!sync.wait()) goto done;
       const int lo = l - 1;  // layer whose pre-activation gradient this is
+      // the saved pre-activations of this row, 32 columns at a time, loaded one
+      // chunk ahead (the first before the wait) to hide their latency
+      const __nv_bfloat16* zrow = a.save + save_z(a.B, lo) + b * H;
+      auto load_z = [&](uint4* z4, int c0) {
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          z4[q] = valid ? *reinterpret_cast<const uint4*>(zrow + c0 + 8 * q) : make_uint4(0u, 0u, 0u, 0u);
+      };
+      uint4 zc[4];
+      load_z(zc, 0);
+      if (!sync.wait()) goto done;
 #pragma unroll 1
       for (int c0 = 0; c0 < H; c0 += 32) {
+        uint4 zn[4];
+        if (c0 + 32 < H) load_z(zn, c0 + 32);
         float v[32];
         umma::tmem_ld32(lane_addr + uint32_t(c0), v);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
           float z[8], d[8];
-          if (valid) unpack8(*reinterpret_cast<const uint4*>(a.save + save_z(a.B, lo) + b * H + c0 + 8 * q), z);
-          else
-#pragma unroll
-            for (int j = 0; j < 8; j++) z[j] = 0.f;
+          unpack8(zc[q], z);
 #pragma unroll
           for (int j = 0; j < 8; j++) d[j] = valid ? v[8 * q + j] * dsilu(z[j]) : 0.f;
           const uint4 dv = pack8(d);
           *reinterpret_cast<uint4*>(s_act + umma::kmaj_off(t, c0 + 8 * q, H)) = dv;
           if (valid) *reinterpret_cast<uint4*>(a.dz + int64_t(lo) * a.B * H + b * H + c0 + 8 * q) = dv;
         }
+#pragma unroll
+        for (int q = 0; q < 4; q++) zc[q] = zn[q];
       }
       umma::fence_before_sync();
       umma::fence_async_shared();
@@ -399,31 +410,46 @@ constexpr int WG_SMEM = 5 * WG_A + 3 * WG_BA + 2 * WG_B16 + 64;
 // TMEM columns of the five accumulators (32-column aligned; 512 allocated)
 constexpr int ACC1 = 0, ACC2 = 160, ACC3 = 320, ACC0 = 480, ACC4 = 496;
 
-// rows [0, 128) of a K-major [rows x K64] tile <- transpose of a [KC][128]
-// row-major BF16 block (rows b0 .. b0+KC of the batch; rows past B are zero)
-__device__ __forceinline__ void stage_t128(uint8_t* dst, const __nv_bfloat16* src, int64_t b0, int64_t B) {
-  const int f = threadIdx.x;  // 128 threads: one output row each
-#pragma unroll 1
-  for (int g = 0; g < KC / 8; g++) {
-    float v[8];
+// Column q (0..7) of an 8 x 8 BF16 block held as 8 rows of 16 bytes: the 8
+// values of that column as 16 bytes (row 0 first).
+__device__ __forceinline__ uint4 column8(const uint4 v[8], int q) {
+  const uint32_t sel = (q & 1) ? 0x7632u : 0x5410u;  // high or low 16-bit half of each word
+  uint32_t w[8];
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const int64_t b = b0 + g * 8 + j;
-      v[j] = b < B ? __bfloat162float(src[b * H + f]) : 0.f;
+  for (int r = 0; r < 8; r++) w[r] = (&v[r].x)[q >> 1];
+  uint4 o;
+  o.x = __byte_perm(w[0], w[1], sel);
+  o.y = __byte_perm(w[2], w[3], sel);
+  o.z = __byte_perm(w[4], w[5], sel);
+  o.w = __byte_perm(w[6], w[7], sel);
+  return o;
+}
+
+// rows [0, F) of a K-major [rows x K64] tile <- transpose of a [KC][F] row-major
+// BF16 block (batch rows b0 .. b0+KC; rows past B are zero). Each task is one
+// 8-feature chunk of 8 consecutive batch rows: eight 16-byte loads, an 8 x 8
+// transpose in registers, eight 16-byte stores of core-matrix rows.
+template <int F>
+__device__ __forceinline__ void stage_t(uint8_t* dst, const __nv_bfloat16* src, int64_t b0, int64_t B) {
+  constexpr int kChunks = F / 8, kTasks = kChunks * (KC / 8);
+  for (int task = threadIdx.x; task < kTasks; task += blockDim.x) {
+    const int ch = task % kChunks, rg = task / kChunks;
+    uint4 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const int64_t b = b0 + rg * 8 + r;
+      v[r] = b < B ? *reinterpret_cast<const uint4*>(src + b * F + ch * 8) : make_uint4(0u, 0u, 0u, 0u);
     }
-    *reinterpret_cast<uint4*>(dst + umma::kmaj_off(f, g * 8, KC)) = pack8(v);
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+      *reinterpret_cast<uint4*>(dst + umma::kmaj_off(ch * 8 + q, rg * 8, KC)) = column8(v, q);
   }
 }
-// 16-row version from a [KC][16] block
+__device__ __forceinline__ void stage_t128(uint8_t* dst, const __nv_bfloat16* src, int64_t b0, int64_t B) {
+  stage_t<H>(dst, src, b0, B);
+}
 __device__ __forceinline__ void stage_t16(uint8_t* dst, const __nv_bfloat16* src, int64_t b0, int64_t B) {
-  const int f = threadIdx.x & 15, g = threadIdx.x >> 4;  // 16 rows x 8 groups
-  float v[8];
-#pragma unroll
-  for (int j = 0; j < 8; j++) {
-    const int64_t b = b0 + g * 8 + j;
-    v[j] = b < B ? __bfloat162float(src[b * 16 + f]) : 0.f;
-  }
-  *reinterpret_cast<uint4*>(dst + umma::kmaj_off(f, g * 8, KC)) = pack8(v);
+  stage_t<16>(dst, src, b0, B);
 }
 
 __global__ void __launch_bounds__(128, 1) mlp_wgrad_kernel(WgArgs a) {
