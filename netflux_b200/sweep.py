@@ -174,6 +174,9 @@ def main(argv=None):
     ap.add_argument("--train-steps", type=int, default=20000)
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--fine-cases", type=int, default=0,
+                    help="additional seeded cases at --fine-nx (closer to the resolution of the 3.1M-tet case)")
+    ap.add_argument("--fine-nx", type=int, default=96)
     ap.add_argument("--eval-pairs", type=int, default=16)
     ap.add_argument("--eval-nx", type=int, default=40)
     ap.add_argument("--out", required=True)
@@ -186,6 +189,8 @@ def main(argv=None):
     summary = {"args": vars(a)}
 
     cases = sample_cases(a.cases, a.seed, a.nx[0], a.nx[1], a.mach, a.h)
+    if a.fine_cases:
+        cases += sample_cases(a.fine_cases, a.seed + 7, a.fine_nx, a.fine_nx, a.mach, a.h)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if world > 1:
