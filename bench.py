@@ -173,7 +173,7 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
 
 
 # DRAM bytes per cell of one launch (dram__bytes_read.sum + dram__bytes_write.sum), captured
-# with ncu on the full 3,145,728-tet bump channel (profiles/dram_traffic_bump3M.md); the bump
+# with ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the full 3,145,728-tet bump channel; the bump
 # workload's `roofline.traffic` is this times its cells, other workloads report null.
 MEASURED_DRAM_BYTES_PER_CELL = {
     ("fp64", "gradient"): 775.1e6 / 3145728, ("fp64", "flux"): 1086.5e6 / 3145728,

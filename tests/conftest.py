@@ -10,4 +10,4 @@ if ROOT not in sys.path:
 
 
 def pytest_configure(config):
-    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (runs on the B200 box)")
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")

@@ -3,8 +3,8 @@
 Run in a checkout that has the reference tree and its build (``make -C
 oracle``): every fixture is produced by oracle/_ref/nf_ref_nodump, the
 reference solver compiled from its own unmodified sources, on small seeded
-meshes from netflux_b200.meshgen. The GPU box has no reference tree, so the
-tests read these files instead.
+meshes from netflux_b200.meshgen. Machines without the reference tree read
+these files instead.
 
     python tests/golden/make_golden.py
 
