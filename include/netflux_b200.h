@@ -234,9 +234,11 @@ int nf_synchronize(nf_solver* s);
 /* Time the launch shapes of the gradient and flux kernels on the current
  * state and keep the fastest: block size (64 or 128 threads), whether each
  * thread issues its next variable's / face's loads before the current
- * arithmetic (variants 1, 3, 5), and a register cap for occupancy (none,
- * variants 0-1; 6 / 8 resident 128-thread blocks for FP64 / FP32, variants
- * 2-3; 7 / 9, variants 4-5). config (may be NULL) receives {gradient block, gradient
+ * arithmetic (variants 1, 3, 5), all of its loads before any arithmetic
+ * (variants 6, 7), or L2 prefetches of its own rows first (variants 8, 9),
+ * and a register cap for occupancy (none, variants 0-1 and 6; 6 / 8 resident
+ * 128-thread blocks for FP64 / FP32, variants 2-3 and 8; 7 / 9, variants 4-5
+ * and 9; 4 / 5, variant 7). config (may be NULL) receives {gradient block, gradient
  * variant, flux block, flux variant}. The state is unchanged. The reference
  * has no counterpart (it runs on one CPU thread). */
 int nf_tune(nf_solver* s, int* config);

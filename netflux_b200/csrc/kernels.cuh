@@ -426,6 +426,21 @@ __global__ void __launch_bounds__(256) flux_update_kernel(MeshView<T> m, StageAr
 // A missing face (a boundary face no marker lists) has S = r = 0 and points
 // at the cell itself, so it changes nothing.
 // ---------------------------------------------------------------------------
+// Ask the memory system to bring a line into L2 without holding a register;
+// the later load of the same address then waits on an L2 hit, not on DRAM.
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+// The own-cell rows the stage update reads (Uin, Un, the local dt).
+__device__ __forceinline__ void prefetch_update_rows(const StageArgs& a, int c, int st) {
+#pragma unroll
+  for (int k = 0; k < 5; k++) prefetch_l2(a.Uin + size_t(k) * st + c);
+  if (a.scheme != 0 && a.stage != 0) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) prefetch_l2(a.Un + size_t(k) * st + c);
+  }
+  if (a.local_dt) prefetch_l2(a.dt_local + c);
+}
+
 template <typename T>
 __device__ __forceinline__ void load_vertices(const MeshView<T>& m, int c, T P[4][3]) {
 #pragma unroll
@@ -459,7 +474,12 @@ __device__ __forceinline__ void face_normals(const T P[4][3], T S[4][3]) {
   face_normal<T, 3>(P, S[3]);
 }
 
-template <typename T, bool kPipe, int kMinBlocks>
+// kPipe: 0 one variable's loads at a time; 1 the next variable's loads in
+// flight during this one's arithmetic; 2 all five variables' loads issued
+// together before any arithmetic (one exposed memory latency instead of five,
+// at the cost of registers); 3 as 0, with the cell's own rows prefetched
+// into L2 first.
+template <typename T, int kPipe, int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView<T> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.n || frozen_cell(a, c)) return;
@@ -477,8 +497,18 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
 #pragma unroll
     for (int q = 0; q < 4; q++) vo[q] = nb[q] >= 0 ? Vk[nb[q]] : Vg[k * m.bstride + (-nb[q] - 1)];
   };
-  T vcN, voN[4];
-  if (kPipe) fetch(0, vcN, voN);
+  if constexpr (kPipe == 3) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) prefetch_l2(Vin + size_t(k) * st + c);
+  }
+  [[maybe_unused]] T vcN, voN[4];
+  [[maybe_unused]] T vcA[5], voA[5][4];
+  if constexpr (kPipe == 2) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) fetch(k, vcA[k], voA[k]);
+  } else if (kPipe == 1) {
+    fetch(0, vcN, voN);
+  }
   const int code = m.gcode[c];
   T S[4][3], d[4][3];  // outward normals; (centroid - P_m) / 3
   {
@@ -503,17 +533,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
                      (S[0][2] + S[1][2]) + (S[2][2] + S[3][2])};
   const T hv = T(0.5) * nr_rcp(T(m.vol[c]));
   const bool rat = a.barth && ratchet_on(a, c);
-#pragma unroll 1
-  for (int k = 0; k < 5; k++) {
-    T vc, vo[4];
-    if (kPipe) {
-      vc = vcN;
-#pragma unroll
-      for (int q = 0; q < 4; q++) vo[q] = voN[q];
-      if (k < 4) fetch(k + 1, vcN, voN);  // next variable's loads overlap this one's arithmetic
-    } else {
-      fetch(k, vc, vo);
-    }
+  auto variable = [&](int k, T vc, const T vo[4]) {
     T acc[3];
 #pragma unroll
     for (int e = 0; e < 3; e++) {
@@ -548,6 +568,24 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
 #pragma unroll
       for (int e = 0; e < 3; e++) a.grad[(k * 3 + e) * st + c] = g[e];
       a.phi[k * st + c] = phi;
+    }
+  };
+  if constexpr (kPipe == 2) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) variable(k, vcA[k], voA[k]);
+  } else {
+#pragma unroll 1
+    for (int k = 0; k < 5; k++) {
+      T vc, vo[4];
+      if (kPipe == 1) {
+        vc = vcN;
+#pragma unroll
+        for (int q = 0; q < 4; q++) vo[q] = voN[q];
+        if (k < 4) fetch(k + 1, vcN, voN);  // next variable's loads overlap this one's arithmetic
+      } else {
+        fetch(k, vc, vo);
+      }
+      variable(k, vc, vo);
     }
   }
 }
@@ -603,7 +641,10 @@ __device__ __forceinline__ void stage_update(const StageArgs& a, int c, int st, 
   else if (!(Vn[0] > 0.0) || !(Vn[4] > 0.0)) atomicOr(a.status, kErrNonPhysical);
 }
 
-template <typename T, bool kPipe, int kMinBlocks>
+// kPipe: 0 one face's loads at a time, 1 the next face's loads in flight
+// during this face's flux, 2 all four faces' loads issued together, 3 as 0
+// with the cell's own face states and update rows prefetched into L2 first.
+template <typename T, int kPipe, int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.n || frozen_cell(a, c)) return;
@@ -636,8 +677,21 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
       }
     }
   };
-  FaceIn<T> nxt;
-  if (kPipe) fetch(0, nxt);
+  if constexpr (kPipe == 3) {
+    if (second) {
+#pragma unroll
+      for (int r = 0; r < 20; r++) prefetch_l2(fsb + size_t(r) * st + c);
+    }
+    prefetch_update_rows(a, c, st);
+  }
+  [[maybe_unused]] FaceIn<T> nxt;
+  [[maybe_unused]] FaceIn<T> all[4];
+  if constexpr (kPipe == 2) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) fetch(q, all[q]);
+  } else if (kPipe == 1) {
+    fetch(0, nxt);
+  }
   T S[4][3];
   {
     T P[4][3];
@@ -648,7 +702,9 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     FaceIn<T> cur;
-    if (kPipe) {
+    if constexpr (kPipe == 2) {
+      cur = all[q];
+    } else if (kPipe == 1) {
       cur = nxt;
       if (q < 3) fetch(q + 1, nxt);  // next face's loads overlap this face's flux
     } else {

@@ -30,23 +30,31 @@ static inline int fast_block(int b) { return b > 128 ? 128 : b; }
 // Variants (the tuner times them): 0 plain, 1 software-pipelined, 2 plain
 // with registers capped for at least kCap resident 128-thread blocks per SM
 // (6 for FP64, 8 for FP32), 3 pipelined with the same cap, 4 and 5 the same
-// with a tighter cap (7 / 9 blocks).
+// with a tighter cap (7 / 9 blocks), 6 and 7 with every load issued before the
+// arithmetic (kPipe 2), uncapped and capped for kCap3 blocks (4 / 5), 8 and 9
+// plain with the cell's own rows prefetched into L2 (kPipe 3), capped as 2
+// and 4. (Prefetching the neighbours' rows as well measured slower.)
 template <typename T>
 constexpr int kCap = sizeof(T) == 8 ? 6 : 8;
-// 4 plain, 5 pipelined, registers capped tighter: at least kCap2 blocks
 template <typename T>
 constexpr int kCap2 = sizeof(T) == 8 ? 7 : 9;
+template <typename T>
+constexpr int kCap3 = sizeof(T) == 8 ? 4 : 5;
 #define NF_NODE_DISPATCH(KERNEL, T, m, a, l)                                                       \
   do {                                                                                              \
     const int b = fast_block(l.block);                                                             \
     const int g = grid_for(m.n, b);                                                                \
     switch (l.variant) {                                                                            \
-      case 1: KERNEL<T, true, 1><<<g, b, 0, l.stream>>>(m, a); break;                             \
-      case 2: KERNEL<T, false, kCap<T>><<<g, b, 0, l.stream>>>(m, a); break;                          \
-      case 3: KERNEL<T, true, kCap<T>><<<g, b, 0, l.stream>>>(m, a); break;                           \
-      case 4: KERNEL<T, false, kCap2<T>><<<g, b, 0, l.stream>>>(m, a); break;                         \
-      case 5: KERNEL<T, true, kCap2<T>><<<g, b, 0, l.stream>>>(m, a); break;                          \
-      default: KERNEL<T, false, 1><<<g, b, 0, l.stream>>>(m, a); break;                           \
+      case 1: KERNEL<T, 1, 1><<<g, b, 0, l.stream>>>(m, a); break;                                 \
+      case 2: KERNEL<T, 0, kCap<T>><<<g, b, 0, l.stream>>>(m, a); break;                           \
+      case 3: KERNEL<T, 1, kCap<T>><<<g, b, 0, l.stream>>>(m, a); break;                           \
+      case 4: KERNEL<T, 0, kCap2<T>><<<g, b, 0, l.stream>>>(m, a); break;                          \
+      case 5: KERNEL<T, 1, kCap2<T>><<<g, b, 0, l.stream>>>(m, a); break;                          \
+      case 6: KERNEL<T, 2, 1><<<g, b, 0, l.stream>>>(m, a); break;                                 \
+      case 7: KERNEL<T, 2, kCap3<T>><<<g, b, 0, l.stream>>>(m, a); break;                          \
+      case 8: KERNEL<T, 3, kCap<T>><<<g, b, 0, l.stream>>>(m, a); break;                           \
+      case 9: KERNEL<T, 3, kCap2<T>><<<g, b, 0, l.stream>>>(m, a); break;                          \
+      default: KERNEL<T, 0, 1><<<g, b, 0, l.stream>>>(m, a); break;                                \
     }                                                                                               \
   } while (0)
 
@@ -62,12 +70,16 @@ void launch_flux_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
     const int b = fast_block(l.block);                                                             \
     const int g = grid_for(m.n, b);                                                                \
     switch (l.variant) {                                                                            \
-      case 1: KERNEL<true, 1><<<g, b, 0, l.stream>>>(m, a); break;                                 \
-      case 2: KERNEL<false, kCap<float>><<<g, b, 0, l.stream>>>(m, a); break;                      \
-      case 3: KERNEL<true, kCap<float>><<<g, b, 0, l.stream>>>(m, a); break;                       \
-      case 4: KERNEL<false, kCap2<float>><<<g, b, 0, l.stream>>>(m, a); break;                     \
-      case 5: KERNEL<true, kCap2<float>><<<g, b, 0, l.stream>>>(m, a); break;                      \
-      default: KERNEL<false, 1><<<g, b, 0, l.stream>>>(m, a); break;                               \
+      case 1: KERNEL<1, 1><<<g, b, 0, l.stream>>>(m, a); break;                                    \
+      case 2: KERNEL<0, kCap<float>><<<g, b, 0, l.stream>>>(m, a); break;                          \
+      case 3: KERNEL<1, kCap<float>><<<g, b, 0, l.stream>>>(m, a); break;                          \
+      case 4: KERNEL<0, kCap2<float>><<<g, b, 0, l.stream>>>(m, a); break;                         \
+      case 5: KERNEL<1, kCap2<float>><<<g, b, 0, l.stream>>>(m, a); break;                         \
+      case 6: KERNEL<2, 1><<<g, b, 0, l.stream>>>(m, a); break;                                    \
+      case 7: KERNEL<2, kCap3<float>><<<g, b, 0, l.stream>>>(m, a); break;                         \
+      case 8: KERNEL<3, kCap<float>><<<g, b, 0, l.stream>>>(m, a); break;                          \
+      case 9: KERNEL<3, kCap2<float>><<<g, b, 0, l.stream>>>(m, a); break;                         \
+      default: KERNEL<0, 1><<<g, b, 0, l.stream>>>(m, a); break;                                   \
     }                                                                                               \
   } while (0)
 

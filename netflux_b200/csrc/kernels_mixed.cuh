@@ -72,7 +72,7 @@ __device__ __forceinline__ void rusanov_delta(const float vc[5], const float dL[
 // Gradient, min/max, Barth limiter (FLT_EPSILON, as the reference's
 // single-precision build, Numerics.hpp:171) and the reconstruction increments
 // phi grad V . r_m, one thread per cell, from FP64 primitives and ghosts.
-template <bool kPipe, int kMinBlocks>
+template <int kPipe, int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshView<float> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.n || frozen_cell(a, c)) return;
@@ -89,8 +89,18 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshVie
 #pragma unroll
     for (int q = 0; q < 4; q++) vo[q] = nb[q] >= 0 ? Vk[nb[q]] : Vg[k * m.bstride + (-nb[q] - 1)];
   };
-  double vcN, voN[4];
-  if (kPipe) fetch(0, vcN, voN);
+  if constexpr (kPipe == 3) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) prefetch_l2(V + size_t(k) * st + c);
+  }
+  [[maybe_unused]] double vcN, voN[4];
+  [[maybe_unused]] double vcA[5], voA[5][4];
+  if constexpr (kPipe == 2) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) fetch(k, vcA[k], voA[k]);
+  } else if (kPipe == 1) {
+    fetch(0, vcN, voN);
+  }
   const int code = m.gcode[c];
   float S[4][3], d[4][3];  // outward normals; (centroid - P_m) / 3
   {
@@ -113,17 +123,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshVie
   }
   const float hv = float(0.5 / m.vol[c]);
   const bool rat = a.barth && ratchet_on(a, c);
-#pragma unroll 1
-  for (int k = 0; k < 5; k++) {
-    double vc, vo[4];
-    if (kPipe) {
-      vc = vcN;
-#pragma unroll
-      for (int q = 0; q < 4; q++) vo[q] = voN[q];
-      if (k < 4) fetch(k + 1, vcN, voN);
-    } else {
-      fetch(k, vc, vo);
-    }
+  auto variable = [&](int k, double vc, const double vo[4]) {
     float dv[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) dv[q] = float(vo[q] - vc);
@@ -169,12 +169,30 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshVie
       for (int e = 0; e < 3; e++) a.grad32[(k * 3 + e) * st + c] = g[e];
       a.phi32[k * st + c] = phi;
     }
+  };
+  if constexpr (kPipe == 2) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) variable(k, vcA[k], voA[k]);
+  } else {
+#pragma unroll 1
+    for (int k = 0; k < 5; k++) {
+      double vc, vo[4];
+      if (kPipe == 1) {
+        vc = vcN;
+#pragma unroll
+        for (int q = 0; q < 4; q++) vo[q] = voN[q];
+        if (k < 4) fetch(k + 1, vcN, voN);
+      } else {
+        fetch(k, vc, vo);
+      }
+      variable(k, vc, vo);
+    }
   }
 }
 
 // Flux balance from the difference form and the FP64 stage update, one
 // thread per cell; boundary faces add boundary_flux_delta_kernel's values.
-template <bool kPipe, int kMinBlocks>
+template <int kPipe, int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) flux_delta_kernel(MeshView<float> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.n || frozen_cell(a, c)) return;
@@ -216,8 +234,21 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_delta_kernel(MeshView<fl
       }
     }
   };
-  FaceIn<float> nxt;
-  if (kPipe) fetch(0, nxt);
+  if constexpr (kPipe == 3) {
+    if (second) {
+#pragma unroll
+      for (int r = 0; r < 20; r++) prefetch_l2(inc + size_t(r) * st + c);
+    }
+    prefetch_update_rows(a, c, st);
+  }
+  [[maybe_unused]] FaceIn<float> nxt;
+  [[maybe_unused]] FaceIn<float> all[4];
+  if constexpr (kPipe == 2) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) fetch(q, all[q]);
+  } else if (kPipe == 1) {
+    fetch(0, nxt);
+  }
   float S[4][3];
   {
     float P[4][3];
@@ -229,7 +260,9 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_delta_kernel(MeshView<fl
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     FaceIn<float> cur;
-    if (kPipe) {
+    if constexpr (kPipe == 2) {
+      cur = all[q];
+    } else if (kPipe == 1) {
       cur = nxt;
       if (q < 3) fetch(q + 1, nxt);
     } else {

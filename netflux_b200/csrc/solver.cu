@@ -397,8 +397,9 @@ struct nf_solver {
       ck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
       return ms;
     };
-    const KCfg cands[] = {{128, 0}, {128, 1}, {128, 2}, {128, 3}, {128, 4}, {128, 5},
-                          {64, 0},  {64, 1},  {64, 2},  {64, 3},  {64, 4},  {64, 5}};
+    const KCfg cands[] = {{128, 0}, {128, 1}, {128, 2}, {128, 3}, {128, 4}, {128, 5}, {128, 6},
+                          {128, 7}, {128, 8}, {128, 9}, {64, 0},  {64, 1},  {64, 2},  {64, 3},
+                          {64, 4},  {64, 5},  {64, 6},  {64, 7},  {64, 8},  {64, 9}};
     if (a.second_order) {
       nf::launch_ghost_fast(view64(), a, launch());
       float best = 1e30f;
@@ -732,7 +733,7 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     s->block = p.block_size > 0 ? p.block_size : 256;
     if (p.block_size > 0) {
       s->kgrad.block = s->kflux.block = std::min(p.block_size, 128);
-      s->kgrad.variant = s->kflux.variant = std::max(0, std::min(p.kernel_variant, 5));
+      s->kgrad.variant = s->kflux.variant = std::max(0, std::min(p.kernel_variant, 9));
       s->tuned = true;  // a caller-fixed shape is not tuned
     }
     if (s->block % 32 || s->block > 256) throw std::runtime_error("block_size must be a multiple of 32, <= 256");

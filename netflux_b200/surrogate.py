@@ -22,6 +22,8 @@ from . import meshgen as mg
 from . import solver as S
 
 GAMMA = 1.4
+# learning-rate pieces of MLP.train_schedule: (fraction of the steps, multiplier)
+LR_SCHEDULE = ((0.5, 1.0), (0.2, 0.3), (0.15, 0.1), (0.15, 0.03))
 # input ranges mapped to [-1, 1]: x, y, z, wall distance, Mach, bump height,
 # and the lower-wall height under the cell, h sin^2(pi (x - 1)) on 1 <= x <= 2
 FEATURE_LO = np.array([0.0, 0.0, 0.0, 0.0, 0.3, 0.05, 0.0])
@@ -64,6 +66,22 @@ class MLP:
         _check(L.load().nf_mlp_train(self._h, int(steps), int(batch), float(lr), int(seed), int(n_report),
                                      L.dptr(rep), C.byref(ms)), self._h)
         return {"loss": rep[:n_report], "ms": ms.value}
+
+    def train_schedule(self, steps: int, batch: int = 65536, lr: float = 1e-3, seed: int = 0,
+                       schedule=None, n_report: int = 20) -> dict:
+        """Adam with a piecewise-constant learning rate: ``schedule`` lists (fraction of the steps,
+        multiplier of lr) pieces; the moments and the step count carry over between pieces."""
+        schedule = LR_SCHEDULE if schedule is None else schedule
+        losses, ms, done = [], 0.0, 0
+        for i, (frac, mult) in enumerate(schedule):
+            n = steps - done if i == len(schedule) - 1 else int(round(frac * steps))
+            if n <= 0:
+                continue
+            r = self.train(n, batch, lr * mult, seed=seed, n_report=max(1, round(n_report * n / max(steps, 1))))
+            losses.extend(np.asarray(r["loss"]).tolist())
+            ms += r["ms"]
+            done += n
+        return {"loss": np.asarray(losses), "ms": ms}
 
     def gradients(self, features: np.ndarray, targets: np.ndarray):
         f = np.ascontiguousarray(features, np.float32)

@@ -174,6 +174,8 @@ def main(argv=None):
     ap.add_argument("--train-steps", type=int, default=20000)
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr-schedule", choices=["step", "constant"], default="step",
+                    help="step: lr, lr/3.3, lr/10, lr/33 over 50/20/15/15 %% of the steps")
     ap.add_argument("--fine-cases", type=int, default=0,
                     help="additional seeded cases at --fine-nx (closer to the resolution of the 3.1M-tet case)")
     ap.add_argument("--fine-nx", type=int, default=96)
@@ -236,8 +238,12 @@ def main(argv=None):
 
     mlp = sur.MLP(seed=a.seed)
     mlp.set_data(F, T)
-    tr = mlp.train(a.train_steps, a.batch, a.lr, seed=a.seed, n_report=20)
+    if a.lr_schedule == "step":
+        tr = mlp.train_schedule(a.train_steps, a.batch, a.lr, seed=a.seed, n_report=20)
+    else:
+        tr = mlp.train(a.train_steps, a.batch, a.lr, seed=a.seed, n_report=20)
     summary["training"] = {"samples": int(F.shape[0]), "steps": a.train_steps, "batch": a.batch, "lr": a.lr,
+                           "lr_schedule": a.lr_schedule,
                            "ms": tr["ms"], "loss": tr["loss"].tolist()}
     np.save(os.path.join(a.out, "mlp_params.npy"), mlp.get_params())
     print(json.dumps({"train_ms": tr["ms"], "loss_first": float(tr["loss"][0]), "loss_last": float(tr["loss"][-1])}),
