@@ -242,6 +242,11 @@ int nf_synchronize(nf_solver* s);
  * variant, flux block, flux variant}. The state is unchanged. The reference
  * has no counterpart (it runs on one CPU thread). */
 int nf_tune(nf_solver* s, int* config);
+/* Fix the launch shapes instead of timing them: config = {gradient block,
+ * gradient variant, flux block, flux variant} as nf_tune reports them (block
+ * 32..128 in steps of 32, variant 0..9); NF_ERR_ARG otherwise. Used to
+ * profile a given shape. No counterpart in the reference. */
+int nf_set_launch_shapes(nf_solver* s, const int* config);
 
 /* Kernel classes reported by nf_time_steps. */
 #define NF_KERNEL_TIMESTEP 0

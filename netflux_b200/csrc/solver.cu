@@ -1455,6 +1455,31 @@ int nf_tune(nf_solver* s, int* config) {
   });
 }
 
+int nf_set_launch_shapes(nf_solver* s, const int* config) {
+  if (!s) return NF_ERR_ARG;
+  return guarded(s, [&]() -> int {
+    if (!config) return NF_ERR_ARG;
+    for (int i = 0; i < 4; i += 2) {
+      const int b = config[i], v = config[i + 1];
+      if (b < 32 || b > 128 || b % 32 || v < 0 || v > 9) {
+        s->err = "launch shapes: block must be 32..128 in steps of 32, variant 0..9";
+        return NF_ERR_ARG;
+      }
+    }
+    s->kgrad.block = config[0];
+    s->kgrad.variant = config[1];
+    s->kflux.block = config[2];
+    s->kflux.variant = config[3];
+    s->tuned = true;
+    for (auto& g : s->graph)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+    return NF_OK;
+  });
+}
+
 int nf_fastmath_selftest(const double* x, int64_t n, double* rcp_out, double* rsqrt_out) {
   if (!x || !rcp_out || !rsqrt_out || n <= 0 || n > (int64_t(1) << 26)) return NF_ERR_ARG;
   try {

@@ -328,6 +328,11 @@ class EulerSolver:
         _check(L.load().nf_tune(self._h, cfg), self._h)
         return {"gradient": {"block": cfg[0], "variant": cfg[1]}, "flux": {"block": cfg[2], "variant": cfg[3]}}
 
+    def set_launch_shapes(self, gradient=(64, 0), flux=(64, 0)):
+        """Fix the gradient/flux launch shapes, each (block, variant) as tune() reports them."""
+        cfg = (C.c_int * 4)(int(gradient[0]), int(gradient[1]), int(flux[0]), int(flux[1]))
+        _check(L.load().nf_set_launch_shapes(self._h, cfg), self._h)
+
     def solve_steady(self, tol: float = 1e-6, max_steps: int = 100000, check_every: int = 50) -> dict:
         """Local-time-stepping steady solve to a relative density-residual drop of ``tol`` (per case)."""
         nc = self.mesh.n_cases

@@ -142,6 +142,16 @@ def test_every_launch_variant_computes_the_same_bits(precision):
             s.advance(3)
             out[(block, variant)] = s.get_solver_data().get_solution()
             s.close()
+    # separate shapes for the two kernels, fixed through nf_set_launch_shapes
+    s = S.EulerSolver(cfg, mesh(g), U0=g["U0"])
+    s.set_launch_shapes(gradient=(64, 7), flux=(128, 9))
+    s.advance(3)
+    out["mixed shapes"] = s.get_solver_data().get_solution()
+    with pytest.raises(L.NetFluxError):
+        s.set_launch_shapes(gradient=(64, 10), flux=(64, 0))
+    with pytest.raises(L.NetFluxError):
+        s.set_launch_shapes(gradient=(64, 0), flux=(200, 0))
+    s.close()
     ref = out[(128, 0)]
     for k, U in out.items():
         assert np.array_equal(U, ref), k
