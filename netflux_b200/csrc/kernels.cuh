@@ -504,8 +504,18 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
   [[maybe_unused]] T vcN, voN[4];
   [[maybe_unused]] T vcA[5], voA[5][4];
   if constexpr (kPipe == 2) {
+    // the same loads as fetch(), with each face's row base and row stride
+    // chosen once (cell row or ghost row) instead of per variable
 #pragma unroll
-    for (int k = 0; k < 5; k++) fetch(k, vcA[k], voA[k]);
+    for (int k = 0; k < 5; k++) vcA[k] = Vin[size_t(k) * st + c];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const bool cell = nb[q] >= 0;
+      const auto* p = cell ? Vin + nb[q] : Vg + (-nb[q] - 1);
+      const size_t rs = cell ? size_t(st) : size_t(m.bstride);
+#pragma unroll
+      for (int k = 0; k < 5; k++) voA[k][q] = p[k * rs];
+    }
   } else if (kPipe == 1) {
     fetch(0, vcN, voN);
   }
