@@ -186,11 +186,12 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
 
 
 # DRAM bytes per cell of one launch (dram__bytes_read.sum + dram__bytes_write.sum), captured
-# with ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the full 3,145,728-tet bump channel; the bump
-# workload's `roofline.traffic` is this times its cells, other workloads report null.
+# with ncu on the full 3,145,728-tet bump channel with the tuned launch shapes (FP64: gradient
+# 64/7, flux 64/9; mixed: gradient 64/7, flux 128/8); the bump workload's `roofline.traffic`
+# is this times its cells, other workloads report null.
 MEASURED_DRAM_BYTES_PER_CELL = {
-    ("fp64", "gradient"): 775.1e6 / 3145728, ("fp64", "flux"): 1086.5e6 / 3145728,
-    ("mixed", "gradient"): 507.9e6 / 3145728, ("mixed", "flux"): 965.7e6 / 3145728,
+    ("fp64", "gradient"): 754.1e6 / 3145728, ("fp64", "flux"): 1100.1e6 / 3145728,
+    ("mixed", "gradient"): 503.7e6 / 3145728, ("mixed", "flux"): 983.6e6 / 3145728,
 }
 
 
