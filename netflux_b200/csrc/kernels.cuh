@@ -441,15 +441,26 @@ __device__ __forceinline__ void prefetch_update_rows(const StageArgs& a, int c, 
   if (a.local_dt) prefetch_l2(a.dt_local + c);
 }
 
+// Node records are 4 values (x, y, z, pad) from a 256-byte aligned buffer, so
+// a record starts on 32 bytes (FP64) or 16 bytes (FP32): x and y come in one
+// 16-byte load (FP64), or the whole record in one (FP32).
 template <typename T>
 __device__ __forceinline__ void load_vertices(const MeshView<T>& m, int c, T P[4][3]) {
 #pragma unroll
   for (int v = 0; v < 4; v++) {
     const int id = m.cnode[v * m.stride + c];
     const T* p = m.nodes + 4 * size_t(id);
-    P[v][0] = p[0];
-    P[v][1] = p[1];
-    P[v][2] = p[2];
+    if constexpr (sizeof(T) == 8) {
+      const double2 xy = *reinterpret_cast<const double2*>(p);
+      P[v][0] = xy.x;
+      P[v][1] = xy.y;
+      P[v][2] = p[2];
+    } else {
+      const float4 r = *reinterpret_cast<const float4*>(p);
+      P[v][0] = r.x;
+      P[v][1] = r.y;
+      P[v][2] = r.z;
+    }
   }
 }
 
@@ -487,7 +498,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
   static_assert(sizeof(T) == 8, "FP64 kernel");
   const T* __restrict__ Vin = a.Vin;
   const T* __restrict__ Vg = a.vg;
-  T* __restrict__ fs = a.fs;
+  T* __restrict__ fsc = a.fs + c;  // this cell's column of the face states
   int nb[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) nb[q] = m.nbvf[q * st + c];
@@ -573,7 +584,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
       if (rat) phi = ratchet(a, size_t(k) * st + c, phi);
     }
 #pragma unroll
-    for (int q = 0; q < 4; q++) fs[(q * 5 + k) * st + c] = fma(phi, gr[q], vc);
+    for (int q = 0; q < 4; q++) fsc[size_t(q * 5 + k) * st] = fma(phi, gr[q], vc);
     if (a.grad) {
 #pragma unroll
       for (int e = 0; e < 3; e++) a.grad[(k * 3 + e) * st + c] = g[e];
@@ -680,10 +691,13 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
     } else {
       const int o = ns[q] >> 2, q2 = ns[q] & 3;
       in.kind = (bits & 4) ? 2 : 1;
+      // row bases chosen once per face: face states (second order) or primitives
+      const T* ps = second ? fsb + size_t(q * 5) * st + c : Vin + c;
+      const T* px = second ? fsb + size_t(q2 * 5) * st + o : Vin + o;
 #pragma unroll
       for (int k = 0; k < 5; k++) {
-        in.s[k] = second ? fsb[(q * 5 + k) * st + c] : Vin[k * st + c];
-        in.x[k] = second ? fsb[(q2 * 5 + k) * st + o] : Vin[k * st + o];
+        in.s[k] = ps[size_t(k) * st];
+        in.x[k] = px[size_t(k) * st];
       }
     }
   };

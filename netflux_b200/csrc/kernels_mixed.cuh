@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshVie
   const int st = m.stride;
   const double* __restrict__ V = a.Vin;
   const double* __restrict__ Vg = a.vg;
-  float* __restrict__ inc_out = a.fs32;
+  float* __restrict__ inc_c = a.fs32 + c;  // this cell's column of the increments
   int nb[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) nb[q] = m.nbvf[q * st + c];
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshVie
       if (rat) phi = ratchet(a, size_t(k) * st + c, phi);
     }
 #pragma unroll
-    for (int q = 0; q < 4; q++) inc_out[(q * 5 + k) * st + c] = phi * gr[q];
+    for (int q = 0; q < 4; q++) inc_c[size_t(q * 5 + k) * st] = phi * gr[q];
     if (a.grad32) {
 #pragma unroll
       for (int e = 0; e < 3; e++) a.grad32[(k * 3 + e) * st + c] = g[e];
@@ -236,11 +236,15 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_delta_kernel(MeshView<fl
     } else {
       const int o = ns[q] >> 2, q2 = ns[q] & 3;
       in.kind = 1;
+      // row bases chosen once per face
+      const double* pv = V + o;
+      const float* ps = inc + size_t(q * 5) * st + c;
+      const float* px = inc + size_t(q2 * 5) * st + o;
 #pragma unroll
       for (int k = 0; k < 5; k++) {
-        const float dvo = float(V[k * st + o] - vcd[k]);
-        in.s[k] = second ? inc[(q * 5 + k) * st + c] : 0.f;
-        in.x[k] = second ? dvo + inc[(q2 * 5 + k) * st + o] : dvo;
+        const float dvo = float(pv[size_t(k) * st] - vcd[k]);
+        in.s[k] = second ? ps[size_t(k) * st] : 0.f;
+        in.x[k] = second ? dvo + px[size_t(k) * st] : dvo;
       }
     }
   };
