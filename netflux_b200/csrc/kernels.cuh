@@ -691,13 +691,10 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
     } else {
       const int o = ns[q] >> 2, q2 = ns[q] & 3;
       in.kind = (bits & 4) ? 2 : 1;
-      // row bases chosen once per face: face states (second order) or primitives
-      const T* ps = second ? fsb + size_t(q * 5) * st + c : Vin + c;
-      const T* px = second ? fsb + size_t(q2 * 5) * st + o : Vin + o;
 #pragma unroll
       for (int k = 0; k < 5; k++) {
-        in.s[k] = ps[size_t(k) * st];
-        in.x[k] = px[size_t(k) * st];
+        in.s[k] = second ? fsb[(q * 5 + k) * st + c] : Vin[k * st + c];
+        in.x[k] = second ? fsb[(q2 * 5 + k) * st + o] : Vin[k * st + o];
       }
     }
   };
