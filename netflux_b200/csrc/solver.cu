@@ -1404,7 +1404,11 @@ int nf_time_steps(nf_solver* s, int64_t n_steps, int per_kernel, double* ms_tota
         ck(cudaGraphInstantiate(&s->graph[v0], g, 0), "graph instantiate");
         cudaGraphDestroy(g);
         s->vcur = v0;
-        // instantiation happened inside the timed region: restart the clock
+        // instantiation happened inside the timed region: upload the graph
+        // (which a first launch would otherwise do while the stream waits),
+        // then restart the clock
+        ck(cudaGraphUpload(s->graph[v0], s->stream), "graph upload");
+        ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
         ck(cudaEventRecord(e0, s->stream), "cudaEventRecord");
       }
       while (left >= 2) {
