@@ -190,8 +190,8 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
 # 64/7, flux 64/9; mixed: gradient 64/7, flux 128/8); the bump workload's `roofline.traffic`
 # is this times its cells, other workloads report null.
 MEASURED_DRAM_BYTES_PER_CELL = {
-    ("fp64", "gradient"): 754.1e6 / 3145728, ("fp64", "flux"): 1100.1e6 / 3145728,
-    ("mixed", "gradient"): 503.7e6 / 3145728, ("mixed", "flux"): 983.6e6 / 3145728,
+    ("fp64", "gradient"): 753.0e6 / 3145728, ("fp64", "flux"): 1099.8e6 / 3145728,
+    ("mixed", "gradient"): 503.2e6 / 3145728, ("mixed", "flux"): 979.7e6 / 3145728,
 }
 
 
