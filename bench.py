@@ -359,15 +359,19 @@ def main():
         pinned = torch.empty((N, 5), dtype=torch.float64, pin_memory=True).numpy()
         pinned[:] = solver.get_solver_data().get_solution()
         n_e = max(1, args.e2e_steps)
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        for _ in range(n_e):
+
+        def e2e_step():
             solver.set_state(pinned)
             solver.calc_timestep(cfg)
             solver.step(cfg)
             rc = lib.nf_get_state(solver._h, L.dptr(pinned), N)
             if rc != 0:
                 raise RuntimeError(L.last_error(solver._h))
+        e2e_step()  # untimed: first use of this host buffer and of the non-graph step path
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(n_e):
+            e2e_step()
         wall = time.perf_counter() - t1
         if dist:
             t = torch.tensor([wall], device="cuda", dtype=torch.float64)
