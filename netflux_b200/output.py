@@ -1,0 +1,75 @@
+"""Solution output for the Python side of the library.
+
+``write_vtk_ascii`` writes the legacy ASCII VTK file that NetFlux's ``Output``
+writes every ``write_stride`` steps (Output.cpp:17-110, file name
+``n=<timestep>.vtk``, Config.hpp:108):
+
+- the grid: ``POINTS`` in file order, ``CELLS`` with each tetrahedron's
+  vertices in the reader's order (vertices 1 and 2 of the SU2 element swapped,
+  GeometryUtilities.cpp:443-466), ``CELL_TYPES`` 10;
+- per cell, ``density``, ``velocity`` (ρu/ρ, ρv/ρ, ρw/ρ) and ``pressure``
+  ((γ−1)(E − 0.5/ρ·|ρu|²), SolverData.hpp:194-201, in that operation order).
+
+Every number is printed as a C++ stream prints a double at its default
+precision (``%g``, 6 significant digits), so the text equals the reference
+program's for the same state.
+
+``snapshot`` pairs with it: ``EulerSolver.snapshot_begin`` starts a copy of the
+state into host memory on a side stream while the solver keeps stepping, and
+``snapshot_wait`` returns it, so output need not stall the step loop.
+"""
+from typing import Optional
+
+import numpy as np
+
+GAMMA_MINUS_ONE = 0.4
+VTK_TETRA = 10
+
+
+def vtk_filename(output_dir: str, timestep: int) -> str:
+    """The reference's name for the file of a time step (Config.hpp:108)."""
+    return output_dir + "n=" + str(int(timestep)) + ".vtk"
+
+
+def _g(a: np.ndarray) -> list:
+    return ["%g" % x for x in np.asarray(a, dtype=np.float64).ravel()]
+
+
+def write_vtk_ascii(path: str, nodes: np.ndarray, reader_tets: np.ndarray, U: np.ndarray,
+                    scalar_name: str = "double", gamma_minus_one: float = GAMMA_MINUS_ONE) -> None:
+    """Write the grid and the cell fields of the conserved state ``U`` [n_cells][5] (reference cell
+    order). ``reader_tets`` holds each cell's vertices in the reader's order
+    (``TetMesh.reader_tets()``)."""
+    nodes = np.asarray(nodes, dtype=np.float64)
+    t = np.asarray(reader_tets, dtype=np.int64)
+    U = np.asarray(U, dtype=np.float64)
+    n_nodes, n_cells = nodes.shape[0], t.shape[0]
+    if U.shape != (n_cells, 5):
+        raise ValueError("state must have shape (n_cells, 5)")
+    rho, m1, m2, m3, E = (U[:, k] for k in range(5))
+    p = gamma_minus_one * (E - 0.5 / rho * ((m1 * m1 + m2 * m2) + m3 * m3))
+    out = ["# vtk DataFile Version 3.0\nNetFlux\nASCII\n\nDATASET UNSTRUCTURED_GRID\n\n",
+           f"POINTS {n_nodes} {scalar_name}\n"]
+    xyz = _g(nodes[:, :3])
+    out.extend(f"{xyz[3 * i]} {xyz[3 * i + 1]} {xyz[3 * i + 2]}\n" for i in range(n_nodes))
+    out.append(f"\nCELLS {n_cells} {n_cells + 4 * n_cells}\n")
+    out.extend("4 " + "".join(f"{v} " for v in row) + "\n" for row in t.tolist())
+    out.append(f"\nCELL_TYPES {n_cells}\n")
+    out.append(f"{VTK_TETRA}\n" * n_cells)
+    out.append(f"\nCELL_DATA {n_cells}\n")
+    out.append(f"\nSCALARS density {scalar_name} 1\nLOOKUP_TABLE default\n")
+    out.extend(s + "\n" for s in _g(rho))
+    out.append(f"\nVECTORS velocity {scalar_name}\n")
+    vel = _g(np.column_stack([m1 / rho, m2 / rho, m3 / rho]))
+    out.extend(f"{vel[3 * i]} {vel[3 * i + 1]} {vel[3 * i + 2]}\n" for i in range(n_cells))
+    out.append(f"\nSCALARS pressure {scalar_name} 1\nLOOKUP_TABLE default\n")
+    out.extend(s + "\n" for s in _g(p))
+    with open(path, "w") as f:
+        f.write("".join(out))
+
+
+def write_solver_vtk(path: str, mesh, solver, U: Optional[np.ndarray] = None) -> None:
+    """Write a solver's current state (or ``U``) on the TetMesh it was built from."""
+    if U is None:
+        U = solver.get_solver_data().get_solution()
+    write_vtk_ascii(path, mesh.nodes, mesh.reader_tets(), U)
