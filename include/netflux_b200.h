@@ -187,6 +187,19 @@ nf_solver* nf_create(const nf_mesh* m, const nf_params* params);
  * the primitives the next nf_calc_timestep reads. */
 int nf_set_state(nf_solver* s, const double* U, int64_t n_cells);
 int nf_get_state(nf_solver* s, double* U, int64_t n_cells);
+/* Start copying the conserved state (reference cell order, [n_cells][5]) to
+ * host memory U without waiting: the copy runs on a side stream and overlaps
+ * the steps queued after this call, which do not change what is copied. U
+ * must stay valid, and unread, until nf_snapshot_wait returns; with pinned
+ * memory (cudaHostAlloc, cudaHostRegister) the copy is asynchronous, with
+ * pageable memory the driver may complete it before returning. One snapshot
+ * is in flight per solver: a second begin first waits for the first. Replaces
+ * the synchronous solution read of Output::write_vtk_ascii (Output.cpp:17-45)
+ * with one the step loop need not wait for. */
+int nf_snapshot_begin(nf_solver* s, double* U, int64_t n_cells);
+/* Wait until the snapshot started by nf_snapshot_begin is in host memory
+ * (NF_OK at once when none is in flight). */
+int nf_snapshot_wait(nf_solver* s);
 /* U^n of the next step's TVD-RK3 combination (the reference's solution_old,
  * Solver.cpp:127-132), AoS [n_cells][5] in reference cell order; applies to
  * the next step only (afterwards U^n is the state, Solver.cpp:51).

@@ -197,6 +197,12 @@ struct nf_solver {
   KCfg kgrad, kflux;
   bool tuned = false;
   DevBuf<double> stage;           // AoS staging for state transfers [N][5]
+  // asynchronous state snapshots (nf_snapshot_begin / nf_snapshot_wait): a
+  // second AoS staging buffer, copied to the host on its own stream
+  DevBuf<double> snap;
+  cudaStream_t snap_stream = nullptr;
+  cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
+  bool snap_pending = false;
   DevBuf<long long> d_dev_of_ref;  // [N]
 
   // per-kernel timing: events around every launch while prof_on
@@ -533,6 +539,10 @@ struct nf_solver {
   }
 
   ~nf_solver() {
+    if (snap_pending) cudaEventSynchronize(snap_done);  // the copy still writes the caller's memory
+    if (snap_ready) cudaEventDestroy(snap_ready);
+    if (snap_done) cudaEventDestroy(snap_done);
+    if (snap_stream) cudaStreamDestroy(snap_stream);
     for (auto& g : graph)
       if (g) cudaGraphExecDestroy(g);
     for (auto e : prof_ev) cudaEventDestroy(e);
@@ -1112,6 +1122,45 @@ int nf_get_state(nf_solver* s, double* U, int64_t n_cells) {
        "U D2H");
     ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
     return s->check_status();
+  });
+}
+
+int nf_snapshot_begin(nf_solver* s, double* U, int64_t n_cells) {
+  return guarded(s, [&]() -> int {
+    if (!U || n_cells != s->n) {
+      s->err = "nf_snapshot_begin: state size does not match the mesh";
+      return NF_ERR_ARG;
+    }
+    if (s->snap_pending) {  // one snapshot in flight per solver
+      ck(cudaEventSynchronize(s->snap_done), "snapshot wait");
+      s->snap_pending = false;
+    }
+    if (!s->snap_stream) {
+      ck(cudaStreamCreateWithFlags(&s->snap_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+      ck(cudaEventCreateWithFlags(&s->snap_ready, cudaEventDisableTiming), "cudaEventCreate");
+      ck(cudaEventCreateWithFlags(&s->snap_done, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    if (s->snap.n != size_t(5) * s->n) s->snap.alloc(size_t(5) * s->n);
+    // the gather is ordered after the queued steps and before the later ones
+    gather_state_kernel<<<(s->n + 255) / 256, 256, 0, s->stream>>>(s->n, s->stride, s->d_dev_of_ref.p, s->U.p,
+                                                                   s->snap.p);
+    ck(cudaGetLastError(), "snapshot gather");
+    ck(cudaEventRecord(s->snap_ready, s->stream), "cudaEventRecord");
+    ck(cudaStreamWaitEvent(s->snap_stream, s->snap_ready, 0), "cudaStreamWaitEvent");
+    ck(cudaMemcpyAsync(U, s->snap.p, size_t(5) * s->n * sizeof(double), cudaMemcpyDeviceToHost, s->snap_stream),
+       "snapshot D2H");
+    ck(cudaEventRecord(s->snap_done, s->snap_stream), "cudaEventRecord");
+    s->snap_pending = true;
+    return NF_OK;
+  });
+}
+
+int nf_snapshot_wait(nf_solver* s) {
+  return guarded(s, [&]() -> int {
+    if (!s->snap_pending) return NF_OK;
+    ck(cudaEventSynchronize(s->snap_done), "snapshot wait");
+    s->snap_pending = false;
+    return NF_OK;
   });
 }
 

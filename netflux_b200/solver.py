@@ -364,10 +364,26 @@ class EulerSolver:
     def get_solver_data(self) -> SolverData:
         return SolverData(self)
 
+    def snapshot_begin(self, out: np.ndarray) -> None:
+        """Start copying the state (reference cell order) into ``out`` while later steps run;
+        ``out`` is a C-contiguous float64 [n_cells][5] array (pinned memory, e.g. a pinned torch
+        tensor's .numpy(), makes the copy asynchronous) and must not be read before snapshot_wait()."""
+        if out.dtype != np.float64 or out.shape != (self.n_cells, 5) or not out.flags.c_contiguous:
+            raise ValueError("snapshot buffer must be a C-contiguous float64 array of shape (n_cells, 5)")
+        _check(L.load().nf_snapshot_begin(self._h, L.dptr(out), self.n_cells), self._h)
+        self._snap = out  # kept alive while the copy runs
+
+    def snapshot_wait(self) -> Optional[np.ndarray]:
+        """Wait for the snapshot in flight and return its array (None when there was none)."""
+        _check(L.load().nf_snapshot_wait(self._h), self._h)
+        out, self._snap = getattr(self, "_snap", None), None
+        return out
+
     def close(self):
         if getattr(self, "_h", None):
-            L.load().nf_destroy(self._h)
+            L.load().nf_destroy(self._h)  # waits for a snapshot in flight
             self._h = None
+        self._snap = None
 
     def __del__(self):
         try:

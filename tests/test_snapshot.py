@@ -1,0 +1,48 @@
+"""Asynchronous state snapshots (nf_snapshot_begin / nf_snapshot_wait) on the GPU: a snapshot taken
+between steps holds exactly the state of that moment although later steps were queued before the
+wait, and the solver's own trajectory is unchanged by it."""
+import numpy as np
+import pytest
+
+from helpers import config_for, golden, mesh
+from netflux_b200 import _lib as L
+from netflux_b200 import solver as S
+
+pytestmark = pytest.mark.gpu
+
+
+def test_snapshot_holds_the_state_of_its_moment():
+    import torch
+    g = golden("bump12")
+    cfg = config_for(precision="fp64", freestream=tuple(g["freestream"]))
+    a = S.EulerSolver(cfg, mesh(g), U0=g["U0"])
+    a.advance(3)
+    ref3 = a.get_solver_data().get_solution()
+    a.advance(4)
+    ref7 = a.get_solver_data().get_solution()
+    a.close()
+
+    b = S.EulerSolver(cfg, mesh(g), U0=g["U0"])
+    b.advance(3)
+    pinned = torch.empty((b.n_cells, 5), dtype=torch.float64, pin_memory=True).numpy()
+    b.snapshot_begin(pinned)
+    b.advance(4)  # queued after the snapshot, before the wait
+    assert b.snapshot_wait() is pinned
+    assert np.array_equal(pinned, ref3)
+    assert np.array_equal(b.get_solver_data().get_solution(), ref7)
+
+    pageable = np.empty((b.n_cells, 5))
+    b.snapshot_begin(pageable)
+    assert np.array_equal(b.snapshot_wait(), ref7)
+    assert b.snapshot_wait() is None  # nothing in flight
+
+    with pytest.raises(ValueError):
+        b.snapshot_begin(np.empty((b.n_cells + 1, 5)))
+    assert L.load().nf_snapshot_begin(b._h, L.dptr(pageable), b.n_cells + 1) == L.NF_ERR_ARG
+
+    b.snapshot_begin(pinned)
+    b.snapshot_begin(pageable)  # the second begin waits for the first
+    b.advance(2)
+    assert np.array_equal(b.snapshot_wait(), ref7)
+    b.snapshot_begin(pinned)
+    b.close()  # destroying the solver waits for the copy in flight
