@@ -14,9 +14,10 @@ Every number is printed as a C++ stream prints a double at its default
 precision (``%g``, 6 significant digits), so the text equals the reference
 program's for the same state.
 
-``snapshot`` pairs with it: ``EulerSolver.snapshot_begin`` starts a copy of the
-state into host memory on a side stream while the solver keeps stepping, and
+``EulerSolver.snapshot_begin`` pairs with it: it starts a copy of the state
+into host memory on a side stream while the solver keeps stepping, and
 ``snapshot_wait`` returns it, so output need not stall the step loop.
+``save_restart`` / ``load_restart`` keep a state with its step count and time.
 """
 from typing import Optional
 
@@ -66,6 +67,26 @@ def write_vtk_ascii(path: str, nodes: np.ndarray, reader_tets: np.ndarray, U: np
     out.extend(s + "\n" for s in _g(p))
     with open(path, "w") as f:
         f.write("".join(out))
+
+
+def save_restart(path: str, U: np.ndarray, timestep: int, time: float = 0.0) -> None:
+    """A restart file: the conserved state [n_cells][5] (reference cell order), the step count and
+    the simulated time. Restoring it with set_state is exact in U; the first time step after it is
+    computed from the restored state's primitives, where an uninterrupted run uses the last stage
+    input's (NetFlux's calc_timestep reads the primitives of the last stage), so the two runs
+    differ from there at the size of one step's change in dt."""
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    if U.ndim != 2 or U.shape[1] != 5:
+        raise ValueError("state must have shape (n_cells, 5)")
+    with open(path, "wb") as f:
+        np.savez(f, U=U, timestep=np.int64(timestep), time=np.float64(time), format=np.int64(1))
+
+
+def load_restart(path: str) -> dict:
+    with np.load(path, allow_pickle=False) as z:
+        if int(z["format"]) != 1:
+            raise ValueError("unknown restart format")
+        return {"U": z["U"].copy(), "timestep": int(z["timestep"]), "time": float(z["time"])}
 
 
 def write_solver_vtk(path: str, mesh, solver, U: Optional[np.ndarray] = None) -> None:

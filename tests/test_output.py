@@ -57,3 +57,14 @@ def test_vtk_rejects_wrong_state_shape(tmp_path):
     m = mg.bump_mesh(2, 1, 1, h=0.1)
     with pytest.raises(ValueError):
         O.write_vtk_ascii(str(tmp_path / "x.vtk"), m.nodes, m.reader_tets(), np.zeros((m.n_cells + 1, 5)))
+
+
+def test_restart_file_round_trips(tmp_path):
+    rng = np.random.default_rng(1)
+    U = rng.random((37, 5))
+    path = str(tmp_path / "r.npz")
+    O.save_restart(path, U, timestep=12, time=0.25)
+    r = O.load_restart(path)
+    assert np.array_equal(r["U"], U) and r["timestep"] == 12 and r["time"] == 0.25
+    with pytest.raises(ValueError):
+        O.save_restart(path, U[:, :4], 0)
