@@ -200,6 +200,19 @@ int nf_snapshot_begin(nf_solver* s, double* U, int64_t n_cells);
 /* Wait until the snapshot started by nf_snapshot_begin is in host memory
  * (NF_OK at once when none is in flight). */
 int nf_snapshot_wait(nf_solver* s);
+/* The other direction: start copying a conserved state (reference cell
+ * order, [n_cells][5]) from host memory U to the device on a side stream,
+ * overlapping the work already queued, which it does not change; U must stay
+ * valid and unchanged until nf_upload_commit returns (pinned memory makes the
+ * copy asynchronous). One upload in flight per solver: a second begin before
+ * the commit is NF_ERR_ARG. nf_upload_commit then makes that state the
+ * solver's state exactly as nf_set_state does, queued after the work already
+ * queued, and returns once the copy has landed; NF_ERR_ARG without a begin.
+ * Together with the snapshots this streams independent states through one
+ * solver with both copies overlapping the steps. No counterpart in the
+ * reference (it has no device memory). */
+int nf_upload_begin(nf_solver* s, const double* U, int64_t n_cells);
+int nf_upload_commit(nf_solver* s);
 /* U^n of the next step's TVD-RK3 combination (the reference's solution_old,
  * Solver.cpp:127-132), AoS [n_cells][5] in reference cell order; applies to
  * the next step only (afterwards U^n is the state, Solver.cpp:51).

@@ -203,6 +203,12 @@ struct nf_solver {
   cudaStream_t snap_stream = nullptr;
   cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
   bool snap_pending = false;
+  // asynchronous state uploads (nf_upload_begin / nf_upload_commit): a third
+  // AoS staging buffer, filled from the host on its own stream
+  DevBuf<double> up;
+  cudaStream_t up_stream = nullptr;
+  cudaEvent_t up_done = nullptr, up_free = nullptr;  // copy landed; scatter done reading `up`
+  bool up_pending = false, up_used = false;
   DevBuf<long long> d_dev_of_ref;  // [N]
 
   // per-kernel timing: events around every launch while prof_on
@@ -538,11 +544,34 @@ struct nf_solver {
     return NF_OK;
   }
 
+  // Make the AoS state in device memory (reference cell order) the solver's
+  // state: permute it into U, primitives of it in both V buffers (the first
+  // calc_timestep reads them, like the harness-initialised reference), and
+  // the step bookkeeping of a fresh start. Queued on the solver stream.
+  void adopt_state(const double* aos) {
+    const int st = stride;
+    scatter_state_kernel<<<(n + 255) / 256, 256, 0, stream>>>(n, st, d_dev_of_ref.p, aos, U.p);
+    for (int b = 0; b < 2; b++) {
+      if (p.precision == NF_PREC_FP64_REF) nf::launch_prim_ref(n, st, U.p, Vbuf(b), nullptr, launch());
+      else nf::launch_prim_fast(n, st, U.p, Vbuf(b), nullptr, launch());
+    }
+    vcur = 0;
+    stepped = false;
+    old_pending = false;
+    steps_done = 0;
+    ratchet_reset();
+    ck(cudaMemsetAsync(status.p, 0, sizeof(unsigned), stream), "status reset");
+  }
+
   ~nf_solver() {
     if (snap_pending) cudaEventSynchronize(snap_done);  // the copy still writes the caller's memory
     if (snap_ready) cudaEventDestroy(snap_ready);
     if (snap_done) cudaEventDestroy(snap_done);
     if (snap_stream) cudaStreamDestroy(snap_stream);
+    if (up_pending) cudaEventSynchronize(up_done);  // the copy still reads the caller's memory
+    if (up_done) cudaEventDestroy(up_done);
+    if (up_free) cudaEventDestroy(up_free);
+    if (up_stream) cudaStreamDestroy(up_stream);
     for (auto& g : graph)
       if (g) cudaGraphExecDestroy(g);
     for (auto e : prof_ev) cudaEventDestroy(e);
@@ -1069,23 +1098,10 @@ int nf_set_state(nf_solver* s, const double* U, int64_t n_cells) {
       s->err = "nf_set_state: state size does not match the mesh";
       return NF_ERR_ARG;
     }
-    const int st = s->stride;
     // one copy of the caller's AoS array, then a permutation kernel into SoA
     ck(cudaMemcpyAsync(s->stage.p, U, size_t(5) * s->n * sizeof(double), cudaMemcpyHostToDevice, s->stream),
        "U H2D");
-    scatter_state_kernel<<<(s->n + 255) / 256, 256, 0, s->stream>>>(s->n, st, s->d_dev_of_ref.p, s->stage.p, s->U.p);
-    // primitives of the initial state in both buffers (the first
-    // calc_timestep reads them, like the harness-initialised reference)
-    for (int b = 0; b < 2; b++) {
-      if (s->p.precision == NF_PREC_FP64_REF) nf::launch_prim_ref(s->n, st, s->U.p, s->Vbuf(b), nullptr, s->launch());
-      else nf::launch_prim_fast(s->n, st, s->U.p, s->Vbuf(b), nullptr, s->launch());
-    }
-    s->vcur = 0;
-    s->stepped = false;
-    s->old_pending = false;
-    s->steps_done = 0;
-    s->ratchet_reset();
-    ck(cudaMemsetAsync(s->status.p, 0, sizeof(unsigned), s->stream), "status reset");
+    s->adopt_state(s->stage.p);
     ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
     ck(cudaGetLastError(), "nf_set_state");
     return NF_OK;
@@ -1160,6 +1176,51 @@ int nf_snapshot_wait(nf_solver* s) {
     if (!s->snap_pending) return NF_OK;
     ck(cudaEventSynchronize(s->snap_done), "snapshot wait");
     s->snap_pending = false;
+    return NF_OK;
+  });
+}
+
+int nf_upload_begin(nf_solver* s, const double* U, int64_t n_cells) {
+  return guarded(s, [&]() -> int {
+    if (!U || n_cells != s->n) {
+      s->err = "nf_upload_begin: state size does not match the mesh";
+      return NF_ERR_ARG;
+    }
+    if (s->up_pending) {
+      s->err = "nf_upload_begin: an upload is already in flight (commit it first)";
+      return NF_ERR_ARG;
+    }
+    if (!s->up_stream) {
+      ck(cudaStreamCreateWithFlags(&s->up_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+      ck(cudaEventCreateWithFlags(&s->up_done, cudaEventDisableTiming), "cudaEventCreate");
+      ck(cudaEventCreateWithFlags(&s->up_free, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    if (s->up.n != size_t(5) * s->n) s->up.alloc(size_t(5) * s->n);
+    // the previous commit's scatter may still be reading the staging buffer
+    if (s->up_used) ck(cudaStreamWaitEvent(s->up_stream, s->up_free, 0), "cudaStreamWaitEvent");
+    ck(cudaMemcpyAsync(s->up.p, U, size_t(5) * s->n * sizeof(double), cudaMemcpyHostToDevice, s->up_stream),
+       "upload H2D");
+    ck(cudaEventRecord(s->up_done, s->up_stream), "cudaEventRecord");
+    s->up_pending = true;
+    return NF_OK;
+  });
+}
+
+int nf_upload_commit(nf_solver* s) {
+  return guarded(s, [&]() -> int {
+    if (!s->up_pending) {
+      s->err = "nf_upload_commit: no upload in flight";
+      return NF_ERR_ARG;
+    }
+    // the solver stream takes the state once the copy has landed; work
+    // queued before this call runs first and is not affected
+    ck(cudaStreamWaitEvent(s->stream, s->up_done, 0), "cudaStreamWaitEvent");
+    s->adopt_state(s->up.p);
+    ck(cudaGetLastError(), "nf_upload_commit");
+    ck(cudaEventRecord(s->up_free, s->stream), "cudaEventRecord");
+    s->up_used = true;
+    ck(cudaEventSynchronize(s->up_done), "upload wait");  // the caller's buffer is free again
+    s->up_pending = false;
     return NF_OK;
   });
 }

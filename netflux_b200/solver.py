@@ -379,11 +379,25 @@ class EulerSolver:
         out, self._snap = getattr(self, "_snap", None), None
         return out
 
+    def upload_begin(self, U: np.ndarray) -> None:
+        """Start copying the state ``U`` (C-contiguous float64 [n_cells][5], reference order) to the
+        device while queued work runs; ``U`` must not change before upload_commit()."""
+        if U.dtype != np.float64 or U.shape != (self.n_cells, 5) or not U.flags.c_contiguous:
+            raise ValueError("upload buffer must be a C-contiguous float64 array of shape (n_cells, 5)")
+        _check(L.load().nf_upload_begin(self._h, L.dptr(U), self.n_cells), self._h)
+        self._up = U  # kept alive while the copy runs
+
+    def upload_commit(self) -> None:
+        """Make the uploaded state the solver's state (as set_state does)."""
+        _check(L.load().nf_upload_commit(self._h), self._h)
+        self._up = None
+
     def close(self):
         if getattr(self, "_h", None):
-            L.load().nf_destroy(self._h)  # waits for a snapshot in flight
+            L.load().nf_destroy(self._h)  # waits for a snapshot or upload in flight
             self._h = None
         self._snap = None
+        self._up = None
 
     def __del__(self):
         try:

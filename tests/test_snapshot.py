@@ -46,3 +46,58 @@ def test_snapshot_holds_the_state_of_its_moment():
     assert np.array_equal(b.snapshot_wait(), ref7)
     b.snapshot_begin(pinned)
     b.close()  # destroying the solver waits for the copy in flight
+
+
+def test_upload_commit_equals_set_state_and_streams_with_snapshots():
+    """nf_upload_begin / nf_upload_commit: a state uploaded while other steps are queued becomes the
+    solver's state exactly as set_state makes it; uploads and snapshots then stream independent
+    states through one solver, both copies overlapping the steps."""
+    import torch
+    g = golden("bump12")
+    cfg = config_for(precision="fp64", freestream=tuple(g["freestream"]))
+    a = S.EulerSolver(cfg, mesh(g), U0=g["U0"])
+    a.advance(2)
+    Ua = a.get_solver_data().get_solution()
+    a.set_state(Ua)
+    a.advance(1)
+    s1 = a.get_solver_data().get_solution()
+    a.advance(2)
+    s3 = a.get_solver_data().get_solution()
+    a.close()
+
+    def pinned(x):
+        t = torch.empty(x.shape, dtype=torch.float64, pin_memory=True).numpy()
+        t[:] = x
+        return t
+
+    ins = [pinned(Ua), pinned(Ua)]
+    b = S.EulerSolver(cfg, mesh(g), U0=g["U0"])
+    b.advance(1)
+    b.upload_begin(ins[0])
+    b.advance(2)  # queued on the old state while the copy runs
+    b.upload_commit()
+    b.advance(3)
+    assert np.array_equal(b.get_solver_data().get_solution(), s3)
+
+    with pytest.raises(L.NetFluxError):
+        b.upload_commit()  # nothing in flight
+    b.upload_begin(ins[0])
+    with pytest.raises(L.NetFluxError):
+        b.upload_begin(ins[1])  # one upload at a time
+    b.upload_commit()
+    assert np.array_equal(b.get_solver_data().get_solution(), Ua)
+    with pytest.raises(ValueError):
+        b.upload_begin(np.empty((b.n_cells, 4)))
+
+    outs = [pinned(np.zeros_like(Ua)), pinned(np.zeros_like(Ua))]
+    b.upload_begin(ins[0])
+    for i in range(4):
+        b.upload_commit()
+        if i < 3:
+            b.upload_begin(ins[(i + 1) % 2])  # the next state's copy overlaps this step
+        b.advance(1)
+        b.snapshot_begin(outs[i % 2])  # this result's copy overlaps the next upload and step
+    b.snapshot_wait()
+    assert np.array_equal(outs[0], s1) and np.array_equal(outs[1], s1)
+    b.upload_begin(ins[0])
+    b.close()  # destroying the solver waits for the upload in flight
