@@ -298,8 +298,9 @@ void nf_destroy(nf_solver* s);
  * is a device pointer to 2 doubles; work is queued on `stream` (a
  * cudaStream_t, NULL for the default stream) and is complete when the stream
  * reaches it. For callers that cannot allocate device memory when they need
- * the reduction (inside CUDA graph capture, under a fixed memory pool, in a
- * real-time loop). Its per-block partial sums live in a fixed 128 KiB array
+ * the reduction (a host that gives the library a fixed memory pool and
+ * forbids allocation after start-up, or a real-time loop that must not block
+ * on the allocator). Its per-block partial sums live in a fixed 128 KiB array
  * in the library, so n is limited to 134,217,728; larger n returns
  * NF_ERR_ARG. The first call on a device looks up that array's address and
  * should come before any stream capture; calls that overlap on the GPU share

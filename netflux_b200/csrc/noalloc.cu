@@ -1,10 +1,9 @@
 // Residual norms with no device allocation.
 //
 // Some callers cannot call cudaMalloc at the point where they need this
-// reduction: code that runs while a CUDA graph is being captured (allocation
-// calls are not capturable), hosts that hand the library a fixed memory pool
-// and forbid allocation after start-up, and real-time drivers that must not
-// block on the allocator. nf_residual_norms_noalloc serves them: the caller
+// reduction: hosts that hand the library a fixed memory pool and forbid
+// allocation after start-up, and real-time drivers that must not block on the
+// allocator (cudaMalloc can synchronise the device). nf_residual_norms_noalloc serves them: the caller
 // passes the input and output device buffers, and the per-block partial sums
 // live in a fixed array compiled into this library.
 //

@@ -1,8 +1,8 @@
 """The allocation-free residual-norm entry point against the solver's own.
 
 nf_residual_norms_noalloc exists for callers that cannot allocate device
-memory when they need the reduction (during CUDA graph capture, under a
-fixed memory pool, in real-time loops); its partial sums live in a fixed array
+memory when they need the reduction (under a fixed memory pool, in real-time
+loops that must not block on the allocator); its partial sums live in a fixed array
 inside the library. This file is collected last so a failure here cannot hide
 any other test, and it passes both on its own and after the rest of the suite.
 """
