@@ -1,0 +1,147 @@
+"""Decomposition of one mesh across ranks (netflux_b200/partition.py), checked on the CPU with the
+oracle standing in for each rank's solver: with the halo exchanged as planned, the owned cells of
+every part evolve as the same cells of the undivided mesh (to round-off: each part sums its faces in
+its own order). Two halo layers carry one stage between exchanges, six carry a TVD-RK3 step."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from netflux_b200 import meshgen as mg
+from netflux_b200 import partition as P
+from netflux_b200 import solver as S
+from oracle import pyoracle as po
+
+RUN = dict(local_time_stepping=True, dt_from_current_state=True, fields=False)
+
+
+def _case():
+    m = mg.bump_mesh(8, 4, 4, h=0.1)
+    fs = mg.bump_freestream(0.5)
+    mm = S.Mesh.from_tet_mesh(m)
+    U0 = mg.uniform_state(mm.n_cells, fs)
+    # a non-uniform start so that gradients and limiters are exercised from the first stage
+    rng = np.random.default_rng(2)
+    U0 = U0 * (1.0 + 0.02 * rng.standard_normal(U0.shape))
+    return m, fs, mm, U0
+
+
+def _global(mm, fs, U0, n_steps, time_scheme):
+    pats = mm.patches()
+    return po.run_oracle(mm.export(), pats, [fs] * len(pats), U0, n_steps, time_scheme=time_scheme, **RUN)["U"]
+
+
+def _rel_linf(a, b):
+    return float(np.max(np.abs(a - b) / np.max(np.abs(b), axis=0)))
+
+
+def test_neighbours_and_halo_layers():
+    m, _, mm, _ = _case()
+    nb = P.cell_neighbours(m.tets)
+    n_interior = int((nb >= 0).sum()) // 2
+    assert n_interior + m.n_boundary_faces == mm.export()["face_ij"].shape[0]
+    rows, cols = np.nonzero(nb >= 0)
+    assert np.all(nb[nb[rows, cols]] .max(axis=1) >= 0)  # every neighbour has neighbours back
+    assert all(rows[i] in nb[nb[rows[i], cols[i]]] for i in range(0, rows.size, 17))
+    parts = P.partition(m, mm.permutation(), 3, layers=2)
+    owned = np.concatenate([p["cells"][:p["n_owned"]] for p in parts])
+    assert np.array_equal(np.sort(owned), np.arange(m.n_cells))
+    for p in parts:
+        level = {c: l for c, l in zip(p["cells"].tolist(), p["layer"].tolist())}
+        for c, l in level.items():
+            if l < 2:  # every neighbour of an owned or first-layer cell is in the part
+                assert all(n < 0 or n in level for n in nb[c])
+        assert np.all(np.diff(p["layer"]) >= 0)
+
+
+@pytest.mark.parametrize("time_scheme,layers,steps_between", [(0, 2, 1), (0, 6, 3), (1, 6, 1)])
+def test_parts_with_exchange_match_the_undivided_mesh(time_scheme, layers, steps_between):
+    m, fs, mm, U0 = _case()
+    n_steps = 6 if time_scheme == 0 else 3
+    ref = _global(mm, fs, U0, n_steps, time_scheme)
+    parts = P.partition(m, mm.permutation(), 3, layers=layers)
+    plan = P.exchange_plan(parts)
+    meshes = [S.Mesh.from_tet_mesh(p["mesh"]) for p in parts]
+    U = [U0[p["cells"]].copy() for p in parts]
+    done = 0
+    while done < n_steps:
+        k = min(steps_between, n_steps - done)
+        for i, mesh in enumerate(meshes):
+            pats = mesh.patches()
+            U[i] = po.run_oracle(mesh.export(), pats, [fs] * len(pats), U[i], k, time_scheme=time_scheme,
+                                 **RUN)["U"]
+        P.exchange(plan, U)
+        done += k
+    out = np.empty_like(U0)
+    for p, u in zip(parts, U):
+        out[p["cells"][:p["n_owned"]]] = u[:p["n_owned"]]
+    assert _rel_linf(out, ref) <= 1e-12
+
+
+def test_too_few_layers_is_not_exact():
+    """The check has teeth: one layer per stage leaves the owned cells at the part edges wrong."""
+    m, fs, mm, U0 = _case()
+    ref = _global(mm, fs, U0, 2, 0)
+    parts = P.partition(m, mm.permutation(), 3, layers=1)
+    plan = P.exchange_plan(parts)
+    U = [U0[p["cells"]].copy() for p in parts]
+    for _ in range(2):
+        for i, p in enumerate(parts):
+            mesh = S.Mesh.from_tet_mesh(p["mesh"])
+            pats = mesh.patches()
+            U[i] = po.run_oracle(mesh.export(), pats, [fs] * len(pats), U[i], 1, time_scheme=0, **RUN)["U"]
+        P.exchange(plan, U)
+    out = np.empty_like(U0)
+    for p, u in zip(parts, U):
+        out[p["cells"][:p["n_owned"]]] = u[:p["n_owned"]]
+    assert _rel_linf(out, ref) > 1e-8
+
+
+def _rank(rank, world, port, out):
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        m, fs, mm, U0 = _case()
+        parts = P.partition(m, mm.permutation(), world, layers=2)
+        plan = P.exchange_plan(parts)
+        me = parts[rank]
+        mesh = S.Mesh.from_tet_mesh(me["mesh"])
+        pats = mesh.patches()
+        U = U0[me["cells"]].copy()
+        for _ in range(4):
+            U = po.run_oracle(mesh.export(), pats, [fs] * len(pats), U, 1, time_scheme=0, **RUN)["U"]
+            reqs, bufs = [], []
+            for q, lists in plan[rank].items():
+                reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(U[lists["send"]])), q))
+            for p in range(world):
+                if rank in plan[p]:
+                    buf = torch.empty((plan[p][rank]["recv"].size, 5), dtype=torch.float64)
+                    reqs.append(dist.irecv(buf, p))
+                    bufs.append((plan[p][rank]["recv"], buf))
+            for r in reqs:
+                r.wait()
+            for idx, buf in bufs:
+                U[idx] = buf.numpy()
+        gathered = [None] * world
+        dist.all_gather_object(gathered, (me["cells"][:me["n_owned"]], U[:me["n_owned"]]))
+        if rank == 0:
+            full = np.empty_like(U0)
+            for cells, u in gathered:
+                full[cells] = u
+            out["err"] = _rel_linf(full, _global(mm, fs, U0, 4, 0))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_exchange_halos():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.spawn(_rank, args=(2, port, out), nprocs=2, join=True)
+    assert out["err"] <= 1e-12
