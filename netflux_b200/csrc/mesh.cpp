@@ -18,10 +18,66 @@
 #include <cstring>
 #include <fstream>
 #include <numeric>
+#include <thread>
 #include <unordered_map>
 
 namespace nf {
 namespace {
+
+// ---- host threads for the large loops and sorts. Every parallel loop writes
+// disjoint elements and every sorted sequence has distinct keys, so the mesh
+// is the same, bit for bit, whatever the thread count. ----
+// NETFLUX_B200_HOST_THREADS (1..64) overrides the thread count (tests use 1
+// to check that the parallel build gives the serial one's mesh)
+int host_threads(size_t n) {
+  if (n < (size_t(1) << 16)) return 1;
+  if (const char* e = std::getenv("NETFLUX_B200_HOST_THREADS")) {
+    const int t = std::atoi(e);
+    if (t >= 1 && t <= 64) return t;
+  }
+  const unsigned hw = std::thread::hardware_concurrency();
+  return int(std::min(16u, std::max(1u, hw)));
+}
+
+// fn(begin, end) over [0, n) in contiguous chunks; fn must not throw
+template <class F>
+void parallel_for(int64_t n, F&& fn) {
+  const int T = host_threads(size_t(n));
+  if (T == 1) {
+    fn(int64_t(0), n);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 0; t < T; t++) {
+    const int64_t b = n * t / T, e = n * (t + 1) / T;
+    th.emplace_back([&fn, b, e] { fn(b, e); });
+  }
+  for (auto& x : th) x.join();
+}
+
+// std::sort of chunks in parallel, then pairwise merges; cmp must be a strict
+// order under which no two elements are equal (so the result is unique)
+template <class T, class Cmp>
+void parallel_sort(std::vector<T>& v, Cmp cmp) {
+  const int P = host_threads(v.size());
+  if (P == 1) {
+    std::sort(v.begin(), v.end(), cmp);
+    return;
+  }
+  std::vector<size_t> cut(size_t(P) + 1);
+  for (int t = 0; t <= P; t++) cut[size_t(t)] = v.size() * size_t(t) / size_t(P);
+  parallel_for(P, [&](int64_t b, int64_t e) {
+    for (int64_t t = b; t < e; t++) std::sort(v.begin() + cut[size_t(t)], v.begin() + cut[size_t(t) + 1], cmp);
+  });
+  for (int w = 1; w < P; w *= 2) {
+    std::vector<std::thread> th;
+    for (int t = 0; t + w < P; t += 2 * w) {
+      const size_t b = cut[size_t(t)], mid = cut[size_t(t + w)], e = cut[size_t(std::min(t + 2 * w, P))];
+      th.emplace_back([&v, &cmp, b, mid, e] { std::inplace_merge(v.begin() + b, v.begin() + mid, v.begin() + e, cmp); });
+    }
+    for (auto& x : th) x.join();
+  }
+}
 
 using V3 = std::array<double, 3>;
 
@@ -95,15 +151,19 @@ void hilbert_renumber(Mesh& m, int64_t begin, int64_t end) {
   if (!(ext > 0)) ext = 1;
   const double q = double((1u << bits) - 1) / ext;
   std::vector<std::pair<uint64_t, int64_t>> keys(size_t(end - begin));
-  for (int64_t c = begin; c < end; c++) {
-    uint32_t u[3];
-    for (int d = 0; d < 3; d++) {
-      double v = (m.centroid[3 * c + d] - lo[d]) * q;
-      u[d] = uint32_t(std::min(std::max(v, 0.0), double((1u << bits) - 1)));
+  parallel_for(end - begin, [&](int64_t k0, int64_t k1) {
+    for (int64_t c = begin + k0; c < begin + k1; c++) {
+      uint32_t u[3];
+      for (int d = 0; d < 3; d++) {
+        double v = (m.centroid[3 * c + d] - lo[d]) * q;
+        u[d] = uint32_t(std::min(std::max(v, 0.0), double((1u << bits) - 1)));
+      }
+      keys[size_t(c - begin)] = {hilbert3(u[0], u[1], u[2], bits), c};
     }
-    keys[size_t(c - begin)] = {hilbert3(u[0], u[1], u[2], bits), c};
-  }
-  std::sort(keys.begin(), keys.end());
+  });
+  parallel_sort(keys, [](const std::pair<uint64_t, int64_t>& x, const std::pair<uint64_t, int64_t>& y) {
+    return x < y;  // (key, cell): distinct
+  });
   for (int64_t k = 0; k < end - begin; k++) {
     m.ref_of_dev[size_t(begin + k)] = keys[size_t(k)].second;
     m.dev_of_ref[size_t(keys[size_t(k)].second)] = begin + k;
@@ -147,7 +207,7 @@ Mesh build_mesh(const std::vector<double>& nodes, const std::vector<int64_t>& te
       // payload: cell (31 bits) and local face (2 bits) in the low 32 bits
       rec[size_t(4 * c + k)] = {(uint64_t(a) << 32) | b, (uint64_t(d) << 32) | (uint64_t(c) << 2 | uint64_t(k))};
     }
-  std::sort(rec.begin(), rec.end(), [](const FaceKey& x, const FaceKey& y) {
+  parallel_sort(rec, [](const FaceKey& x, const FaceKey& y) {  // lo carries (cell, face): distinct
     return x.hi != y.hi ? x.hi < y.hi : x.lo < y.lo;
   });
 
@@ -181,8 +241,8 @@ Mesh build_mesh(const std::vector<double>& nodes, const std::vector<int64_t>& te
   }
   rec.clear();
   rec.shrink_to_fit();
-  std::sort(interior.begin(), interior.end(), [](const IFace& x, const IFace& y) {
-    return x.i != y.i ? x.i < y.i : x.j < y.j;  // Faces::sort (GeometryUtilities.cpp:484-513)
+  parallel_sort(interior, [](const IFace& x, const IFace& y) {
+    return x.i != y.i ? x.i < y.i : x.j < y.j;  // Faces::sort (GeometryUtilities.cpp:484-513); two tets share one face at most
   });
 
   // ---- boundary faces: markers in file order, ghosts numbered in that order ----
@@ -285,12 +345,15 @@ Mesh build_mesh(const std::vector<double>& nodes, const std::vector<int64_t>& te
     m.face_i[size_t(f)] = i;
     m.face_j[size_t(f)] = j;
   };
-  for (int64_t f = 0; f < NIF; f++) {
-    const IFace& x = interior[size_t(f)];
-    uint32_t fn[3];
-    for (int q = 0; q < 3; q++) fn[q] = tet[size_t(4 * x.i + kTetFace[x.k][q])];
-    face_geometry(f, x.i, x.j, fn);
-  }
+  // interior faces write only their own face's entries (j < N: no ghost centroid)
+  parallel_for(NIF, [&](int64_t f0, int64_t f1) {
+    for (int64_t f = f0; f < f1; f++) {
+      const IFace& x = interior[size_t(f)];
+      uint32_t fn[3];
+      for (int q = 0; q < 3; q++) fn[q] = tet[size_t(4 * x.i + kTetFace[x.k][q])];
+      face_geometry(f, x.i, x.j, fn);
+    }
+  });
   int64_t f = NIF;
   for (size_t p = 0; p < markers.size(); p++) {
     Patch P;

@@ -123,3 +123,19 @@ def test_concat_offsets_and_patches():
     assert list(c.case_offsets()) == [0, a.n_cells, a.n_cells + b.n_cells]
     assert [p["case"] for p in c.patches()] == [0] * len(a.patches()) + [1] * len(b.patches())
     assert c.n_faces == a.n_faces + b.n_faces
+
+
+def test_parallel_build_equals_serial_build(monkeypatch):
+    """The builder's threaded sorts and loops (meshes above 65,536 face records) give the mesh the
+    one-thread build gives, bit for bit."""
+    m = mg.bump_mesh(40, 20, 20, h=0.1)  # 96,000 tets: every parallel path runs
+    out = []
+    for threads in ("1", "7"):
+        monkeypatch.setenv("NETFLUX_B200_HOST_THREADS", threads)
+        mm = S.Mesh.from_tet_mesh(m)
+        out.append((mm.export(), mm.permutation(), mm.patches()))
+    (a, pa, qa), (b, pb, qb) = out
+    assert set(a) == set(b)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(pa, pb) and qa == qb
