@@ -1,9 +1,11 @@
-"""Parity at the full sizes of the two CPU-runnable workloads:
+"""Parity at the full sizes of the workloads:
   * unit cube, 20^3 hexes x 6 tets (48,000 cells), Gaussian density bump, far field all round,
     TVD-RK3 at CFL 0.8: against the compiled reference (or the oracle where it is not built),
     FP64 <= 1e-12 after 1 step and <= 1e-9 after 100 steps;
   * Sod tube, 400 x 8 x 8 hexes x 6 tets (153,600 cells), slip sides, far-field ends, to t = 0.2:
-    FP64 and mixed against the reference-order form, itself pinned to the oracle at this size.
+    FP64 and mixed against the reference-order form, itself pinned to the oracle at this size;
+  * the bump channel, 128 x 64 x 64 hexes x 6 tets (3,145,728 cells), by size-independent
+    properties (repeatability, launch shapes, mixed against FP64).
 Errors are relative L-infinity with the momentum components scaled by max |rho u| (helpers.rel_linf)."""
 import os
 import tempfile
@@ -93,3 +95,37 @@ def test_config2_sod_153k_cells_to_t_0_2():
     assert pin <= 1e-13
     assert e["fp64"][0] <= 1e-9
     assert e["mixed"][0] <= 1e-3 and e["mixed"][1] <= 1e-5
+
+
+def test_config3_bump_3m_cells_properties():
+    """The 3,145,728-tet channel (the bench workload), one TVD-RK3 step with local time stepping from
+    a smoothly perturbed free stream. It is too large for the oracle, so it is checked by properties
+    that do not depend on size: a second run repeats every bit, the tuned launch shapes change no
+    bit, and the mixed form stays within its 1e-5 bar of FP64."""
+    m = mg.bump_mesh(128, 64, 64, h=0.1)
+    fs = mg.bump_freestream(0.5)
+    mesh = S.Mesh.from_tet_mesh(m)
+    assert mesh.n_cells == 3145728
+    c = m.centroids()
+    V = np.broadcast_to(np.asarray(fs, np.float64), (mesh.n_cells, 5)).copy()
+    bump = 0.02 * np.sin(2 * np.pi * c[:, 0] / 3.0) * np.sin(np.pi * c[:, 1]) * np.sin(np.pi * c[:, 2])
+    V[:, 0] *= 1.0 + bump
+    V[:, 4] *= 1.0 + 0.5 * bump
+    U0 = mg.prim_to_cons(V)
+    a = _gpu(mesh, U0, "fp64", 1, fs, local_time_stepping=True)
+    b = _gpu(mesh, U0, "fp64", 1, fs, local_time_stepping=True)
+    assert np.array_equal(a, b)
+    cfg = S.Config(precision="fp64", CFL=0.8, density_fs=fs[0], velocity_fs=list(fs[1:4]), pressure_fs=fs[4],
+                   local_time_stepping=True)
+    s = S.EulerSolver(cfg, mesh, U0=U0)
+    s.tune()
+    s.set_state(U0)
+    s.advance(1)
+    assert np.array_equal(s.get_solver_data().get_solution(), a)
+    s.close()
+    mixed = _gpu(mesh, U0, "mixed", 1, fs, local_time_stepping=True)
+    err = rel_linf(mixed, a)
+    print("config 3, mixed vs FP64 after 1 step: %.2e; max change of the step %.2e"
+          % (err, rel_linf(a, U0)))
+    assert err <= 1e-5
+    assert rel_linf(a, U0) > 1e-6  # the step did change the state
