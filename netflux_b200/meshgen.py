@@ -299,6 +299,62 @@ def write_su2(path: str, mesh: TetMesh) -> None:
                 f.write("\n")
 
 
+def read_su2(path: str, patch_types: Dict[str, str]) -> TetMesh:
+    """Read an SU2 tetrahedral mesh as NetFlux's reader does (PrimalGrid.cpp:140-244): element lines
+    are "10 n0 n1 n2 n3" with anything after the nodes ignored, node coordinates are read as a
+    stream of three numbers per node, and marker elements are "5 n0 n1 n2" triangles. Only
+    tetrahedra are accepted (other volume elements are rejected, as in this library's builder).
+    ``patch_types`` maps every marker name to its boundary type ("FarField", "SlipWall",
+    "NoSlipWall"); the TetMesh keeps the file's node order of every element."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    pos = 0
+
+    def next_line():
+        nonlocal pos
+        while pos < len(lines) and not lines[pos].strip():
+            pos += 1
+        if pos >= len(lines):
+            raise ValueError("unexpected end of the mesh file")
+        pos += 1
+        return lines[pos - 1].split()
+
+    def keyword(want):
+        tok = next_line()
+        if len(tok) < 2 or tok[0] != want:
+            raise ValueError(f"symbol '{tok[0] if tok else ''}' parsed instead of correct symbol '{want}'")
+        return tok[1]
+
+    if int(keyword("NDIME=")) != 3:
+        raise ValueError("only three dimensions (NDIME= 3) are accepted")
+    n_elem = int(keyword("NELEM="))
+    tets = np.empty((n_elem, 4), np.int64)
+    for i in range(n_elem):
+        tok = next_line()
+        if int(tok[0]) != 10:
+            raise ValueError(f"element {i}: only tetrahedra (10) are supported, got {tok[0]}")
+        tets[i] = [int(t) for t in tok[1:5]]
+    n_nodes = int(keyword("NPOIN="))
+    vals: List[float] = []
+    while len(vals) < 3 * n_nodes:  # a stream of numbers, three per node
+        vals.extend(float(t) for t in next_line())
+    nodes = np.array(vals[:3 * n_nodes], np.float64).reshape(n_nodes, 3)
+    markers = []
+    for _ in range(int(keyword("NMARK="))):
+        name = keyword("MARKER_TAG=")
+        k = int(keyword("MARKER_ELEMS="))
+        tris = np.empty((k, 3), np.int64)
+        for i in range(k):
+            tok = next_line()
+            if int(tok[0]) != 5:
+                raise ValueError(f"marker '{name}' element {i}: only triangles (5) are supported")
+            tris[i] = [int(t) for t in tok[1:4]]
+        if name not in patch_types:
+            raise ValueError(f"marker '{name}' has no boundary type")
+        markers.append((name, tris))
+    return TetMesh(nodes=nodes, tets=tets, markers=markers, patch_types=dict(patch_types))
+
+
 def input_yml_text(patch_types: Dict[str, str], freestream, cfl: float = 0.8,
                    n_timesteps: int = 1, time_scheme: str = "TVD_RK3",
                    spatial_order: str = "Second", limiter: str = "Barth",

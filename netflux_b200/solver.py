@@ -407,22 +407,63 @@ class EulerSolver:
 
 
 class Driver:
-    """Driver::solve (Driver.cpp:24-61) for one solver, without output."""
+    """Driver::solve (Driver.cpp:24-61) for one solver: calc_timestep and step until n_timesteps.
 
-    def __init__(self, config: Config, U0: Optional[np.ndarray] = None):
+    With ``write_output`` it also writes what NetFlux's Output writes: the VTK file of the state at
+    step 0 and at every ``write_stride``-th step (Output::write_vtk_ascii, Output.cpp:17-45) into
+    ``<sim_dir>/output/``, which it first empties as Output's constructor does (Output.cpp:3-14).
+
+    Without ``U0`` it starts as NetFlux's program does: the free stream in ``solution`` and
+    ``solution_old`` left at zero (SolverData.cpp:50-58), which the first TVD-RK3 step combines with
+    (Solver.cpp:127-132). ``solver`` and ``tet_mesh`` may be given instead of being built from the
+    configuration's SU2 file."""
+
+    def __init__(self, config: Config, U0: Optional[np.ndarray] = None, write_output: bool = False,
+                 solver=None, tet_mesh=None):
+        from . import meshgen as mg
         self.config = config
-        self.mesh = Mesh.from_su2(config.get_mesh_filename_path(), config.patch_bc)
-        self.solver = EulerSolver(config, self.mesh, U0)
+        self.write_output = write_output
+        if tet_mesh is None and write_output:
+            types = {name: next(t for t, c in mg.BC_CODES.items() if c == code)
+                     for name, code in config.patch_bc.items()}
+            tet_mesh = mg.read_su2(config.get_mesh_filename_path(), types)
+        self.tet_mesh = tet_mesh
+        if solver is None:
+            self.mesh = Mesh.from_su2(config.get_mesh_filename_path(), config.patch_bc)
+            solver = EulerSolver(config, self.mesh, U0)
+            if U0 is None:
+                solver.set_state_old(np.zeros((self.mesh.n_cells, 5)))
+        self.solver = solver
+        if write_output:
+            import shutil
+            out = self.output_dir()
+            if os.path.exists(out):
+                shutil.rmtree(out)
+            os.makedirs(out)
+
+    def output_dir(self) -> str:
+        return self.config.sim_dir + "output/"  # Config::get_output_dir (Config.hpp:106)
+
+    def _write(self) -> None:
+        cfg = self.config
+        if not self.write_output or cfg.get_timestep() % cfg.write_stride != 0:
+            return
+        from . import output
+        U = self.solver.get_solver_data().get_solution()
+        output.write_vtk_ascii(output.vtk_filename(self.output_dir(), cfg.get_timestep()), self.tet_mesh.nodes,
+                               self.tet_mesh.reader_tets(), U)
 
     def solve(self) -> None:
         cfg = self.config
         cfg.set_timestep(0)
         cfg.set_time(0.0)
+        self._write()
         while True:
             self.solver.calc_timestep(cfg)
             self.solver.step(cfg)
             cfg.set_timestep(cfg.get_timestep() + 1)
             cfg.set_time(cfg.get_time() + cfg.get_delta_time())
+            self._write()
             if cfg.get_timestep() >= cfg.get_n_timesteps():
                 break
         self.solver.synchronize()
