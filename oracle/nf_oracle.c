@@ -251,6 +251,78 @@ static int timestep(const nfo_mesh* m, const nfo_params* p, const double* V, dou
   return 0;
 }
 
+/* Stage s of explicit Euler / TVD-RK3 from the flux balance in w->R
+ * (Solver.cpp:83-133): U is the stage input and receives the output. */
+static void stage_update(const nfo_mesh* m, const nfo_params* p, const work_t* w, double* U, const double* Un, int s,
+                         double dt, const double* dtl) {
+  for (int64_t i = 0; i < w->NC; i++) {
+    const double h = dtl ? dtl[i] : dt;
+    for (int k = 0; k < 5; k++) {
+      double* u = U + 5 * i + k;
+      const double r = w->R[5 * i + k];
+      if (p->time_scheme == 0 || s == 0) /* Solver.cpp:97-98, 123-124 */
+        *u += h / m->vol[i] * r;
+      else if (s == 1) /* Solver.cpp:127-128 */
+        *u = 3.0 / 4.0 * Un[5 * i + k] + 1.0 / 4.0 * *u + 1.0 / 4.0 * h / m->vol[i] * r;
+      else /* Solver.cpp:131-132 */
+        *u = 1.0 / 3.0 * Un[5 * i + k] + 2.0 / 3.0 * *u + 2.0 / 3.0 * h / m->vol[i] * r;
+    }
+  }
+}
+
+static void free_work(work_t* w) {
+  free(w->V);
+  free(w->G);
+  free(w->L);
+  free(w->Vmax);
+  free(w->Vmin);
+  free(w->R);
+  free(w->face_patch);
+  free(w->Lf);
+}
+
+int nfo_timestep_of(const nfo_mesh* m, const nfo_params* p, const double* U, double* dt_out, double* dtl) {
+  if (!m || !p || !U || !dt_out || m->n_cells <= 0) return 2;
+  double* V = (double*)malloc(sizeof(double) * 5 * m->n_cells);
+  if (!V) return 2;
+  for (int64_t i = 0; i < m->n_cells; i++) cons_to_prim(U + 5 * i, V + 5 * i);
+  const int rc = timestep(m, p, V, dt_out, dtl);
+  free(V);
+  return rc;
+}
+
+int nfo_stage(const nfo_mesh* m, const nfo_params* p, double* U, const double* Un, int stage, double dt,
+              const double* dtl) {
+  if (!m || !p || !U || !Un || m->n_cells <= 0 || m->n_faces < m->n_interior_faces || stage < 0 || stage > 2 ||
+      p->limiter_ratchet_step > 0)
+    return 2;
+  work_t w;
+  memset(&w, 0, sizeof w);
+  w.NC = m->n_cells;
+  w.NF = m->n_faces;
+  w.NIF = m->n_interior_faces;
+  w.NT = w.NC + (w.NF - w.NIF);
+  w.V = (double*)calloc((size_t)(5 * w.NT), sizeof(double));
+  w.G = (double*)calloc((size_t)(15 * w.NC), sizeof(double));
+  w.L = (double*)calloc((size_t)(5 * w.NC), sizeof(double));
+  w.Vmax = (double*)calloc((size_t)(5 * w.NC), sizeof(double));
+  w.Vmin = (double*)calloc((size_t)(5 * w.NC), sizeof(double));
+  w.R = (double*)calloc((size_t)(5 * w.NC), sizeof(double));
+  w.face_patch = (int*)calloc((size_t)w.NF, sizeof(int));
+  int rc = 0;
+  if (!w.V || !w.G || !w.L || !w.Vmax || !w.Vmin || !w.R || !w.face_patch) {
+    rc = 2;
+  } else {
+    g_density_fix = p->farfield_density_fix;
+    for (int q = 0; q < m->n_patches; q++)
+      for (int64_t f = m->patch_first[q]; f < m->patch_first[q] + m->patch_n[q]; f++) w.face_patch[f] = q;
+    flux_balance(m, p, &w, U);
+    stage_update(m, p, &w, U, Un, stage, dt, dtl);
+  }
+  free_work(&w);
+  return rc;
+}
+
 int nfo_run(const nfo_mesh* m, const nfo_params* p, double* U, int64_t n_steps, double* dt_hist, double* V_out,
             double* grad_out, double* lim_out, double* R_out, double* res_out, double* time_out) {
   if (!m || !p || !U || m->n_cells <= 0 || m->n_faces < m->n_interior_faces) return 2;
@@ -316,19 +388,7 @@ int nfo_run(const nfo_mesh* m, const nfo_params* p, double* U, int64_t n_steps, 
         res_out[2 * n] = sqrt(ss / (double)w.NC);
         res_out[2 * n + 1] = mx;
       }
-      for (int64_t i = 0; i < w.NC; i++) {
-        const double h = dtl ? dtl[i] : dt;
-        for (int k = 0; k < 5; k++) {
-          double* u = U + 5 * i + k;
-          const double r = w.R[5 * i + k];
-          if (p->time_scheme == 0 || s == 0) /* Solver.cpp:97-98, 123-124 */
-            *u += h / m->vol[i] * r;
-          else if (s == 1) /* Solver.cpp:127-128 */
-            *u = 3.0 / 4.0 * Un[5 * i + k] + 1.0 / 4.0 * *u + 1.0 / 4.0 * h / m->vol[i] * r;
-          else /* Solver.cpp:131-132 */
-            *u = 1.0 / 3.0 * Un[5 * i + k] + 2.0 / 3.0 * *u + 2.0 / 3.0 * h / m->vol[i] * r;
-        }
-      }
+      stage_update(m, p, &w, U, Un, s, dt, dtl);
     }
     memcpy(Un, U, sizeof(double) * 5 * w.NC); /* solution_old = solution (Solver.cpp:51) */
     time += dt;

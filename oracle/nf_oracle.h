@@ -63,6 +63,19 @@ typedef struct {
 int nfo_run(const nfo_mesh* m, const nfo_params* p, double* U, int64_t n_steps, double* dt_hist, double* V_out,
             double* grad_out, double* lim_out, double* R_out, double* res_out, double* time_out);
 
+/* Pieces of a step, for tests that split a step across ranks and exchange
+ * halo states between stages (extension; same arithmetic as nfo_run):
+ * nfo_timestep_of computes calc_timestep from the primitives of U (the
+ * dt_from_current_state form): the minimum in dt_out and, when dtl is not
+ * NULL, the per-cell values. nfo_stage runs stage `stage` (0..2; 0 only for
+ * explicit Euler) on U (stage input in, stage output out) with Un the step's
+ * starting state and the step's dt, or the per-cell dtl when not NULL. The
+ * limiter ratchet is not supported there (2). Both return 0, 5 for an
+ * invalid dt, 2 on bad input. */
+int nfo_timestep_of(const nfo_mesh* m, const nfo_params* p, const double* U, double* dt_out, double* dtl);
+int nfo_stage(const nfo_mesh* m, const nfo_params* p, double* U, const double* Un, int stage, double dt,
+              const double* dtl);
+
 #ifdef __cplusplus
 }
 #endif

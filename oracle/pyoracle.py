@@ -50,6 +50,12 @@ def _load():
         _lib.nfo_run.restype = C.c_int
         _lib.nfo_run.argtypes = [C.POINTER(_Mesh), C.POINTER(_Params), C.POINTER(C.c_double), C.c_int64] + \
             [C.POINTER(C.c_double)] * 7
+        _lib.nfo_timestep_of.restype = C.c_int
+        _lib.nfo_timestep_of.argtypes = [C.POINTER(_Mesh), C.POINTER(_Params), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        _lib.nfo_stage.restype = C.c_int
+        _lib.nfo_stage.argtypes = [C.POINTER(_Mesh), C.POINTER(_Params), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_double), C.c_int, C.c_double, C.POINTER(C.c_double)]
     return _lib
 
 
@@ -98,6 +104,53 @@ def run_oracle(grid: Dict[str, np.ndarray], patches: Sequence[dict], patch_fs: S
     out["res"] = out["res"][:n_steps]
     out["time"] = float(out["time"][0])
     return out
+
+
+class StageOracle:
+    """Single stages of the C restatement on one grid (extension for tests that split a step across
+    ranks and exchange halo states between stages): ``timestep`` is calc_timestep from the current
+    state's primitives, ``stage`` one explicit-Euler / TVD-RK3 stage with a given dt."""
+
+    def __init__(self, grid: Dict[str, np.ndarray], patches: Sequence[dict], patch_fs: Sequence[Sequence[float]],
+                 time_scheme: int = 1, spatial_order: int = 1, limiter: int = 1, cfl: float = 0.8,
+                 local_time_stepping: bool = False):
+        self._lib = _load()
+        F = grid["face_ij"].shape[0]
+        self.NC = grid["dS"].shape[0]
+        NG = grid["vol"].shape[0] - self.NC
+        self._keep = {k: np.ascontiguousarray(grid[k]) for k in ("face_ij", "S", "ri", "rj", "vol", "dS")}
+        self._ptype = np.array([p["type"] for p in patches], np.int32)
+        self._pfirst = np.array([p["first_face"] for p in patches], np.int64)
+        self._pn = np.array([p["n_faces"] for p in patches], np.int64)
+        self._pfs = np.ascontiguousarray(np.asarray(patch_fs, np.float64).reshape(len(patches), 5))
+        k = self._keep
+        self._m = _Mesh(self.NC, F, F - NG, k["face_ij"].ctypes.data_as(C.POINTER(C.c_uint32)), _dp(k["S"]),
+                        _dp(k["ri"]), _dp(k["rj"]), _dp(k["vol"]), _dp(k["dS"]), len(patches),
+                        self._ptype.ctypes.data_as(C.POINTER(C.c_int)),
+                        self._pfirst.ctypes.data_as(C.POINTER(C.c_int64)),
+                        self._pn.ctypes.data_as(C.POINTER(C.c_int64)), _dp(self._pfs))
+        self.lts = bool(local_time_stepping)
+        self._p = _Params(time_scheme, spatial_order, limiter, int(local_time_stepping), 1, cfl, 0.0, 0, 0, None)
+
+    def timestep(self, U: np.ndarray):
+        """(global dt, per-cell dt or None) from the primitives of U."""
+        U = np.ascontiguousarray(U, np.float64)
+        dt = C.c_double()
+        dtl = np.empty(self.NC) if self.lts else None
+        rc = self._lib.nfo_timestep_of(C.byref(self._m), C.byref(self._p), _dp(U), C.byref(dt), _dp(dtl))
+        if rc != 0:
+            raise RuntimeError(f"oracle timestep failed with code {rc}")
+        return dt.value, dtl
+
+    def stage(self, U: np.ndarray, Un: np.ndarray, stage: int, dt: float, dtl: Optional[np.ndarray]) -> np.ndarray:
+        out = np.ascontiguousarray(U, np.float64).copy()
+        Un = np.ascontiguousarray(Un, np.float64)
+        dtl = np.ascontiguousarray(dtl, np.float64) if dtl is not None else None
+        rc = self._lib.nfo_stage(C.byref(self._m), C.byref(self._p), _dp(out), _dp(Un), int(stage), float(dt),
+                                 _dp(dtl))
+        if rc != 0:
+            raise RuntimeError(f"oracle stage failed with code {rc}")
+        return out
 
 
 def reference_available(variant: str = "nf_ref_nodump") -> bool:

@@ -1,7 +1,8 @@
 """Decomposition of one mesh across ranks (netflux_b200/partition.py), checked on the CPU with the
 oracle standing in for each rank's solver: with the halo exchanged as planned, the owned cells of
 every part evolve as the same cells of the undivided mesh (to round-off: each part sums its faces in
-its own order). Two halo layers carry one stage between exchanges, six carry a TVD-RK3 step."""
+its own order). Two halo layers carry one stage between exchanges (explicit Euler steps, or TVD-RK3
+stages through the oracle's stage entry points), six carry a TVD-RK3 step."""
 import os
 import socket
 
@@ -76,6 +77,36 @@ def test_parts_with_exchange_match_the_undivided_mesh(time_scheme, layers, steps
                                  **RUN)["U"]
         P.exchange(plan, U)
         done += k
+    out = np.empty_like(U0)
+    for p, u in zip(parts, U):
+        out[p["cells"][:p["n_owned"]]] = u[:p["n_owned"]]
+    assert _rel_linf(out, ref) <= 1e-12
+
+
+@pytest.mark.parametrize("global_dt", [False, True])
+def test_rk3_with_two_layers_and_an_exchange_per_stage(global_dt):
+    """The production plan: 2 halo layers, the halo states exchanged after every TVD-RK3 stage, and
+    with a global time step the minimum taken over the owned cells of all parts (an all-reduce)."""
+    m, fs, mm, U0 = _case()
+    pats = mm.patches()
+    ref = po.run_oracle(mm.export(), pats, [fs] * len(pats), U0, 3, time_scheme=1,
+                        local_time_stepping=not global_dt, dt_from_current_state=True, fields=False)["U"]
+    parts = P.partition(m, mm.permutation(), 3, layers=2)
+    plan = P.exchange_plan(parts)
+    so = []
+    for p in parts:
+        mesh = S.Mesh.from_tet_mesh(p["mesh"])
+        pp = mesh.patches()
+        so.append(po.StageOracle(mesh.export(), pp, [fs] * len(pp), time_scheme=1, local_time_stepping=True))
+    U = [U0[p["cells"]].copy() for p in parts]
+    for _ in range(3):
+        dts = [o.timestep(u) for o, u in zip(so, U)]
+        dt_g = min(float(np.min(dtl[:p["n_owned"]])) for (_, dtl), p in zip(dts, parts))
+        Un = [u.copy() for u in U]
+        for stage in range(3):
+            U = [o.stage(u, un, stage, dt_g, None) if global_dt else o.stage(u, un, stage, 0.0, dtl)
+                 for o, u, un, (_, dtl) in zip(so, U, Un, dts)]
+            P.exchange(plan, U)
     out = np.empty_like(U0)
     for p, u in zip(parts, U):
         out[p["cells"][:p["n_owned"]]] = u[:p["n_owned"]]
