@@ -78,10 +78,22 @@ def run_sharded(cases: List[Dict], rank: int, world: int, gather, run=None, **kw
     return merged, res, parts[rank]
 
 
+def build_case_meshes(cases: List[Dict], threads: int = 0) -> List[S.Mesh]:
+    """The cases' meshes, built on host threads (the mesh generator and the library's builder
+    release the interpreter for most of their work); the list is in case order and each mesh is
+    the one a serial build gives."""
+    from concurrent.futures import ThreadPoolExecutor
+    n = threads or min(16, os.cpu_count() or 1)
+    if n <= 1 or len(cases) <= 1:
+        return [case_mesh(c) for c in cases]
+    with ThreadPoolExecutor(max_workers=min(n, len(cases))) as ex:
+        return list(ex.map(case_mesh, cases))
+
+
 def run_batched(cases: List[Dict], precision: str = "mixed", tol: float = 1e-6, max_steps: int = 400000,
                 check_every: int = 100, device: int = -1) -> Dict:
     t0 = time.perf_counter()
-    meshes = [case_mesh(c) for c in cases]
+    meshes = build_case_meshes(cases)
     fss = [mg.bump_freestream(c["mach"]) for c in cases]
     batch = S.Mesh.concat(meshes)
     t_mesh = time.perf_counter() - t0

@@ -53,3 +53,13 @@ def test_two_ranks_shard_and_gather():
     for i, r in enumerate(m0):
         assert r["nx"] == cases[i]["nx"] and r["steps"] == 100 + cases[i]["nx"]
         assert r["rank"] == (0 if i in mine0 else 1)
+
+
+def test_threaded_case_meshes_equal_serial_ones():
+    cases = SW.sample_cases(6, 5, 8, 14)
+    serial = SW.build_case_meshes(cases, threads=1)
+    threaded = SW.build_case_meshes(cases, threads=4)
+    for a, b in zip(serial, threaded):
+        ea, eb = a.export(), b.export()
+        assert a.n_cells == b.n_cells and all(np.array_equal(ea[k], eb[k]) for k in ea)
+        assert np.array_equal(a.permutation(), b.permutation())
