@@ -176,3 +176,17 @@ def test_two_gloo_ranks_exchange_halos():
     out = mgr.dict()
     mp.spawn(_rank, args=(2, port, out), nprocs=2, join=True)
     assert out["err"] <= 1e-12
+
+
+def test_partition_edge_cases():
+    m, _, mm, _ = _case()
+    one = P.partition(m, mm.permutation(), 1, layers=2)
+    assert one[0]["n_owned"] == m.n_cells and one[0]["cells"].size == m.n_cells  # no halo
+    assert P.exchange_plan(one) == {0: {}}
+    bare = P.partition(m, mm.permutation(), 4, layers=0)
+    assert all(p["cells"].size == p["n_owned"] for p in bare)
+    assert sum(p["n_owned"] for p in bare) == m.n_cells
+    with pytest.raises(ValueError):
+        P.partition(m, mm.permutation(), 0)
+    with pytest.raises(ValueError):
+        P.partition(m, mm.permutation(), 2, layers=-1)
