@@ -182,6 +182,9 @@ typedef struct {
 
 void nf_params_default(nf_params* p);
 
+/* One solver takes at most 107,374,080 cells (its kernels use 32-bit row
+ * offsets); a larger mesh is refused with a message (nf_last_error(NULL)) and
+ * is split across solvers instead. */
 nf_solver* nf_create(const nf_mesh* m, const nf_params* params);
 /* U in reference cell order, AoS [n_cells][5]. Setting the state also sets
  * the primitives the next nf_calc_timestep reads. */

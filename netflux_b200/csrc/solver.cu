@@ -150,6 +150,10 @@ namespace nf {
 void set_last_error_text(const std::string& msg) { g_create_error = msg; }
 }  // namespace nf
 
+// Largest cell count one solver takes: 20 rows of (N rounded up to 64) int
+// offsets must stay below 2^31 (107,374,080 cells).
+constexpr int64_t kMaxCells = (int64_t(INT32_MAX) / 20) / 64 * 64 - 64;
+
 struct nf_solver {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -783,6 +787,11 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
 
     const int64_t N = m.n_cells, F = m.n_faces;
     if (N >= (int64_t(1) << 30) || F >= (int64_t(1) << 30)) throw std::runtime_error("mesh too large for one solver");
+    // The stage kernels index the 20 face-state rows of [20][stride] arrays
+    // with 32-bit products, so 20 * stride must stay below 2^31.
+    if (N > kMaxCells)
+      throw std::runtime_error("mesh too large for one solver: at most " + std::to_string(kMaxCells) +
+                               " cells (split larger meshes across solvers)");
     s->n = int(N);
     s->stride = int((N + 63) / 64 * 64);
     s->n_faces = int(F);
