@@ -312,6 +312,24 @@ void nf_destroy(nf_solver* s);
 int nf_residual_norms_noalloc(const double* values, int64_t n, double* out, void* stream);
 
 
+/* Cap on the host threads one mesh build (nf_mesh_from_su2 / _from_arrays /
+ * _concat) uses: 0 restores the default (the hardware's threads, at most 16),
+ * n in 1..64 bounds it. For callers that build several meshes at once on
+ * their own threads, so that builds times builder threads do not oversubscribe
+ * the host. Process-wide; the environment variable NETFLUX_B200_HOST_THREADS,
+ * when set, takes precedence. No reference counterpart (its grid builder is
+ * single-threaded). */
+int nf_set_host_threads(int n);
+
+/* Whether one solver can take a mesh of n_cells interior cells and n_faces
+ * faces: NF_OK, or NF_ERR_MESH with the reason in nf_last_error(NULL).
+ * nf_create applies the same check. The stage kernels address the 20 rows of
+ * the [20][stride] face-state arrays with 32-bit offsets (stride = n_cells
+ * rounded up to 64), so at most 107,374,080 cells fit one solver; larger
+ * meshes are split across solvers. No reference counterpart (the reference's
+ * arrays are 64-bit indexed). */
+int nf_check_mesh_size(int64_t n_cells, int64_t n_faces);
+
 /* Self-test of the fast forms' reciprocal and reciprocal square root (a
  * single-precision estimate refined by two Newton-Raphson steps) on n
  * positive inputs; no reference counterpart. */

@@ -10,6 +10,8 @@
 // reference's (no fused multiply-add on the x86-64 baseline it targets).
 #include "mesh.hpp"
 
+#include "../../include/netflux_b200.h"
+
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -18,6 +20,7 @@
 #include <cstring>
 #include <fstream>
 #include <numeric>
+#include <atomic>
 #include <thread>
 #include <unordered_map>
 
@@ -28,7 +31,11 @@ namespace {
 // disjoint elements and every sorted sequence has distinct keys, so the mesh
 // is the same, bit for bit, whatever the thread count. ----
 // NETFLUX_B200_HOST_THREADS (1..64) overrides the thread count (tests use 1
-// to check that the parallel build gives the serial one's mesh)
+// to check that the parallel build gives the serial one's mesh); a cap set by
+// nf_set_host_threads (callers that build several meshes at once on their own
+// threads) bounds the default.
+std::atomic<int> g_thread_cap{0};
+
 int host_threads(size_t n) {
   if (n < (size_t(1) << 16)) return 1;
   if (const char* e = std::getenv("NETFLUX_B200_HOST_THREADS")) {
@@ -36,7 +43,10 @@ int host_threads(size_t n) {
     if (t >= 1 && t <= 64) return t;
   }
   const unsigned hw = std::thread::hardware_concurrency();
-  return int(std::min(16u, std::max(1u, hw)));
+  int t = int(std::min(16u, std::max(1u, hw)));
+  const int cap = g_thread_cap.load(std::memory_order_relaxed);
+  if (cap > 0) t = std::min(t, cap);
+  return t;
 }
 
 // fn(begin, end) over [0, n) in contiguous chunks; fn must not throw
@@ -562,3 +572,9 @@ Mesh concat_meshes(const std::vector<const Mesh*>& parts) {
 }
 
 }  // namespace nf
+
+extern "C" int nf_set_host_threads(int n) {
+  if (n < 0 || n > 64) return NF_ERR_ARG;
+  nf::g_thread_cap.store(n, std::memory_order_relaxed);
+  return NF_OK;
+}

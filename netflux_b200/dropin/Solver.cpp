@@ -39,6 +39,11 @@ using namespace geometry;
 
 namespace {
 
+// Device solver of each live Solver object. The reference's Solver has no
+// destructor this file could define (Solver.hpp declares none, and Driver
+// destroys it through its implicit one), so an entry outlives its Solver: its
+// device memory is released when a new Solver takes the same address (the old
+// object is then gone) or at exit. NetFlux's Driver creates one Solver per run.
 // Never destroyed, so the exit handler below can still walk it.
 std::map<const Solver*, nf_solver*>& table() {
   static auto* t = new std::map<const Solver*, nf_solver*>;
@@ -168,6 +173,8 @@ EulerSolver::EulerSolver(const Config& config, const PrimalGrid& primal_grid, co
   if (!s) throw std::runtime_error(std::string("netflux_b200: ") + nf_last_error(nullptr));
   static const bool registered = (std::atexit(release_all) == 0);
   (void)registered;
+  auto stale = table().find(this);
+  if (stale != table().end()) nf_destroy(stale->second);  // a destroyed Solver's, at this address
   table()[this] = s;
   const VecField& U = solver_data->get_solution();  // free stream (SolverData.cpp:50-58)
   check(nf_set_state(s, U[0], int64_t(U.size())), s);

@@ -69,24 +69,54 @@ def write_vtk_ascii(path: str, nodes: np.ndarray, reader_tets: np.ndarray, U: np
         f.write("".join(out))
 
 
-def save_restart(path: str, U: np.ndarray, timestep: int, time: float = 0.0) -> None:
+def mesh_fingerprint(mesh) -> str:
+    """SHA-256 of a Mesh's face grid in the reference's order (face cell pairs, face normals and cell
+    volumes) and its case offsets: two meshes with the same fingerprint give the same step."""
+    import hashlib
+    g = mesh.export()
+    h = hashlib.sha256()
+    for k in ("face_ij", "S", "vol"):
+        h.update(np.ascontiguousarray(g[k]).tobytes())
+    h.update(np.ascontiguousarray(mesh.case_offsets(), np.int64).tobytes())
+    return h.hexdigest()
+
+
+def save_restart(path: str, U: np.ndarray, timestep: int, time: float = 0.0, mesh=None) -> None:
     """A restart file: the conserved state [n_cells][5] (reference cell order), the step count and
-    the simulated time. Restoring it with set_state is exact in U; the first time step after it is
+    the simulated time; with ``mesh`` (a solver.Mesh) also its fingerprint and case offsets, which
+    load_restart checks. Restoring it with set_state is exact in U; the first time step after it is
     computed from the restored state's primitives, where an uninterrupted run uses the last stage
     input's (NetFlux's calc_timestep reads the primitives of the last stage), so the two runs
     differ from there at the size of one step's change in dt."""
     U = np.ascontiguousarray(U, dtype=np.float64)
     if U.ndim != 2 or U.shape[1] != 5:
         raise ValueError("state must have shape (n_cells, 5)")
+    extra = {}
+    if mesh is not None:
+        if mesh.n_cells != U.shape[0]:
+            raise ValueError("state size does not match the mesh")
+        extra = {"mesh_sha256": np.array(mesh_fingerprint(mesh)),
+                 "case_offsets": np.ascontiguousarray(mesh.case_offsets(), np.int64)}
     with open(path, "wb") as f:
-        np.savez(f, U=U, timestep=np.int64(timestep), time=np.float64(time), format=np.int64(1))
+        np.savez(f, U=U, timestep=np.int64(timestep), time=np.float64(time), format=np.int64(2), **extra)
 
 
-def load_restart(path: str) -> dict:
+def load_restart(path: str, mesh=None) -> dict:
+    """Read a restart file; with ``mesh`` the file must have been written for that mesh (same
+    fingerprint and case offsets, when the file records them) or ValueError is raised."""
     with np.load(path, allow_pickle=False) as z:
-        if int(z["format"]) != 1:
+        if int(z["format"]) not in (1, 2):
             raise ValueError("unknown restart format")
-        return {"U": z["U"].copy(), "timestep": int(z["timestep"]), "time": float(z["time"])}
+        out = {"U": z["U"].copy(), "timestep": int(z["timestep"]), "time": float(z["time"])}
+        if "mesh_sha256" in z.files:
+            out["mesh_sha256"] = str(z["mesh_sha256"])
+            out["case_offsets"] = z["case_offsets"].copy()
+    if mesh is not None:
+        if out["U"].shape[0] != mesh.n_cells:
+            raise ValueError("restart file was written for a mesh of another size")
+        if "mesh_sha256" in out and out["mesh_sha256"] != mesh_fingerprint(mesh):
+            raise ValueError("restart file was written for a different mesh")
+    return out
 
 
 def write_solver_vtk(path: str, mesh, solver, U: Optional[np.ndarray] = None) -> None:

@@ -115,15 +115,26 @@ def sub_mesh(mesh: TetMesh, cells: np.ndarray) -> TetMesh:
 
 
 def _search_rows(sorted_rows: np.ndarray, rows: np.ndarray) -> np.ndarray:
-    """Index of each row of ``rows`` in the lexicographically sorted ``sorted_rows``, or -1."""
-    if sorted_rows.shape[0] == 0:
-        return np.full(rows.shape[0], -1, np.int64)
-    base = max(int(sorted_rows.max()), int(rows.max())) + 1
-    key_s = (sorted_rows[:, 0] * base + sorted_rows[:, 1]) * base + sorted_rows[:, 2]
-    key_r = (rows[:, 0] * base + rows[:, 1]) * base + rows[:, 2]
-    i = np.searchsorted(key_s, key_r)
-    i = np.minimum(i, key_s.size - 1)
-    return np.where(key_s[i] == key_r, i, -1)
+    """Index of each row of ``rows`` in the lexicographically sorted ``sorted_rows`` (its first
+    occurrence), or -1. Rows are merged and compared column by column, never packed into one
+    integer key, so any int64 values work (node ids of meshes of any size)."""
+    sorted_rows = np.asarray(sorted_rows, dtype=np.int64)
+    rows = np.asarray(rows, dtype=np.int64)
+    n, m = sorted_rows.shape[0], rows.shape[0]
+    res = np.full(m, -1, np.int64)
+    if n == 0 or m == 0:
+        return res
+    allr = np.concatenate([sorted_rows, rows])
+    tag = np.concatenate([np.zeros(n, np.int64), np.ones(m, np.int64)])
+    # stable: within a run of equal rows the sorted rows come first, in their own order
+    order = np.lexsort((tag,) + tuple(allr[:, k] for k in range(allr.shape[1] - 1, -1, -1)))
+    r = allr[order]
+    starts = np.ones(n + m, bool)
+    starts[1:] = np.any(r[1:] != r[:-1], axis=1)
+    first = order[np.maximum.accumulate(np.where(starts, np.arange(n + m), 0))]  # first row of each run
+    hit = (order >= n) & (first < n)
+    res[order[hit] - n] = first[hit]
+    return res
 
 
 def exchange_plan(parts: List[Dict[str, np.ndarray]]) -> Dict[int, Dict[int, Dict[str, np.ndarray]]]:

@@ -27,6 +27,7 @@ from typing import Dict, List
 import numpy as np
 
 from . import meshgen as mg
+from . import _lib as L
 from . import solver as S
 from . import surrogate as sur
 
@@ -81,13 +82,21 @@ def run_sharded(cases: List[Dict], rank: int, world: int, gather, run=None, **kw
 def build_case_meshes(cases: List[Dict], threads: int = 0) -> List[S.Mesh]:
     """The cases' meshes, built on host threads (the mesh generator and the library's builder
     release the interpreter for most of their work); the list is in case order and each mesh is
-    the one a serial build gives."""
+    the one a serial build gives. The host's cores are split between the builds: with w builds at
+    once each builder uses at most cores / w threads of its own (nf_set_host_threads)."""
     from concurrent.futures import ThreadPoolExecutor
-    n = threads or min(16, os.cpu_count() or 1)
+    cores = os.cpu_count() or 1
+    n = threads or min(16, cores)
     if n <= 1 or len(cases) <= 1:
         return [case_mesh(c) for c in cases]
-    with ThreadPoolExecutor(max_workers=min(n, len(cases))) as ex:
-        return list(ex.map(case_mesh, cases))
+    workers = min(n, len(cases))
+    lib = L.load()
+    lib.nf_set_host_threads(max(1, cores // workers))
+    try:
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            return list(ex.map(case_mesh, cases))
+    finally:
+        lib.nf_set_host_threads(0)
 
 
 def run_batched(cases: List[Dict], precision: str = "mixed", tol: float = 1e-6, max_steps: int = 400000,

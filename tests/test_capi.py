@@ -28,6 +28,21 @@ def test_library_exports_every_declared_symbol():
     assert set(names) == set(L.EXPORTED)
 
 
+def test_mesh_size_limit_of_one_solver():
+    """The largest mesh one solver takes (32-bit offsets into the 20 face-state rows): 107,374,080
+    cells; one more is refused with a message, as nf_create refuses it."""
+    lib = L.load()
+    k_max = (2 ** 31 - 1) // 20 // 64 * 64 - 64
+    assert k_max == 107374080
+    assert 20 * ((k_max + 63) // 64 * 64) < 2 ** 31
+    assert lib.nf_check_mesh_size(k_max, 2 * k_max) == L.NF_OK
+    assert lib.nf_check_mesh_size(k_max + 1, 2 * k_max) == L.NF_ERR_MESH
+    assert "at most 107374080" in L.last_error(None)
+    assert lib.nf_check_mesh_size(1, 0) == L.NF_OK
+    assert lib.nf_check_mesh_size(0, 0) == L.NF_ERR_MESH
+    assert lib.nf_check_mesh_size(1000, 2 ** 30) == L.NF_ERR_MESH
+
+
 def test_params_default():
     p = L.NfParams()
     L.load().nf_params_default(C.byref(p))

@@ -68,3 +68,22 @@ def test_restart_file_round_trips(tmp_path):
     assert np.array_equal(r["U"], U) and r["timestep"] == 12 and r["time"] == 0.25
     with pytest.raises(ValueError):
         O.save_restart(path, U[:, :4], 0)
+
+
+def test_restart_file_records_and_checks_its_mesh(tmp_path):
+    from netflux_b200 import solver as S
+    a = S.Mesh.from_tet_mesh(mg.bump_mesh(4, 2, 2, h=0.1))
+    b = S.Mesh.from_tet_mesh(mg.bump_mesh(4, 2, 2, h=0.05))  # same size, other geometry
+    U = np.random.default_rng(2).random((a.n_cells, 5))
+    path = str(tmp_path / "r.npz")
+    O.save_restart(path, U, timestep=3, time=0.5, mesh=a)
+    r = O.load_restart(path, mesh=a)
+    assert np.array_equal(r["U"], U) and r["mesh_sha256"] == O.mesh_fingerprint(a)
+    assert r["case_offsets"].tolist() == [0, a.n_cells]
+    with pytest.raises(ValueError, match="different mesh"):
+        O.load_restart(path, mesh=b)
+    c = S.Mesh.from_tet_mesh(mg.bump_mesh(6, 2, 2, h=0.1))
+    with pytest.raises(ValueError, match="size"):
+        O.load_restart(path, mesh=c)
+    with pytest.raises(ValueError):
+        O.save_restart(path, U[:-1], 0, mesh=a)

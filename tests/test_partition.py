@@ -190,3 +190,37 @@ def test_partition_edge_cases():
         P.partition(m, mm.permutation(), 0)
     with pytest.raises(ValueError):
         P.partition(m, mm.permutation(), 2, layers=-1)
+
+
+def test_search_rows_matches_brute_force_for_large_ids():
+    """Rows are matched column by column: ids far above 2^21 (where three ids no longer pack into
+    one int64) still find their rows, first occurrence first."""
+    rng = np.random.default_rng(5)
+    base = np.array([2 ** 40, 2 ** 39, 2 ** 41], np.int64)
+    rows = base + rng.integers(0, 4, (300, 3))
+    srt = rows[np.lexsort((rows[:, 2], rows[:, 1], rows[:, 0]))]
+    queries = np.concatenate([rows[:50], base + rng.integers(3, 6, (50, 3))])
+    got = P._search_rows(srt, queries)
+    for q, g in zip(queries, got):
+        eq = np.nonzero(np.all(srt == q, axis=1))[0]
+        assert g == (eq[0] if eq.size else -1)
+    assert P._search_rows(srt[:0], queries).tolist() == [-1] * len(queries)
+    assert P._search_rows(srt, queries[:0]).size == 0
+
+
+def test_sub_mesh_with_node_ids_above_2_21_keeps_every_marker():
+    """The same mesh with 3,000,000 unused nodes in front of its own: the part meshes keep the same
+    boundary triangles (an int64 key of three packed ids would overflow here and drop them)."""
+    m = mg.box_tet_mesh(4, 3, 3, jitter=0.1, seed=3)
+    off = 3_000_000
+    nodes = np.zeros((off + m.nodes.shape[0], 3))
+    nodes[off:] = m.nodes
+    big = mg.TetMesh(nodes=nodes, tets=np.asarray(m.tets, np.int64) + off,
+                     markers=[(n, np.asarray(t, np.int64) + off) for n, t in m.markers],
+                     patch_types=dict(m.patch_types))
+    cells = np.arange(0, m.n_cells, 3)
+    a, b = P.sub_mesh(m, cells), P.sub_mesh(big, cells)
+    assert np.array_equal(a.tets, b.tets)
+    assert sum(t.shape[0] for _, t in a.markers) > 0
+    for (na, ta), (nb_, tb) in zip(a.markers, b.markers):
+        assert na == nb_ and np.array_equal(ta, tb)
