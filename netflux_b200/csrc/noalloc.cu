@@ -43,6 +43,10 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 double* g_partials_addr[kMaxDevices] = {};
 
+// max(a, b) that keeps a NaN from either operand (fmax would drop it: a
+// non-finite value must show in the max norm).
+__device__ __forceinline__ double max_keep_nan(double a, double b) { return (a != a || a > b) ? a : b; }
+
 __global__ void __launch_bounds__(kThreads) partials_kernel(const double* __restrict__ v, long long n,
                                                             double* __restrict__ part) {
   const long long beg = blockIdx.x * kChunk;
@@ -51,7 +55,7 @@ __global__ void __launch_bounds__(kThreads) partials_kernel(const double* __rest
   for (long long i = beg + threadIdx.x; i < end; i += kThreads) {
     const double x = v[i];
     s += x * x;
-    mx = fmax(mx, fabs(x));
+    mx = max_keep_nan(mx, fabs(x));
   }
   __shared__ double ss[kThreads], sm[kThreads];
   ss[threadIdx.x] = s;
@@ -60,7 +64,7 @@ __global__ void __launch_bounds__(kThreads) partials_kernel(const double* __rest
   for (int w = kThreads / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) {
       ss[threadIdx.x] += ss[threadIdx.x + w];
-      sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+      sm[threadIdx.x] = max_keep_nan(sm[threadIdx.x], sm[threadIdx.x + w]);
     }
     __syncthreads();
   }
@@ -75,7 +79,7 @@ __global__ void finalize_kernel(const double* __restrict__ part, int n_blocks, l
   double s = 0.0, mx = 0.0;
   for (int b = 0; b < n_blocks; b++) {  // fixed order: deterministic
     s += part[2 * b];
-    mx = fmax(mx, part[2 * b + 1]);
+    mx = max_keep_nan(mx, part[2 * b + 1]);
   }
   out[0] = n > 0 ? sqrt(s / double(n)) : 0.0;
   out[1] = mx;

@@ -80,6 +80,10 @@ __global__ void scal_kernel(double* scal, int op, unsigned* status) {
   }
 }
 
+// max(a, b) that keeps a NaN from either operand (fmax would drop it, and a
+// non-finite residual must not vanish from the L-infinity norm).
+__device__ __forceinline__ double max_keep_nan(double a, double b) { return (a != a || a > b) ? a : b; }
+
 // Per-case RMS and max of the per-cell density residual (deterministic: fixed
 // chunking, fixed summation order).
 __global__ void residual_partials_kernel(const double* __restrict__ r, const long long* __restrict__ chunk_begin,
@@ -90,7 +94,7 @@ __global__ void residual_partials_kernel(const double* __restrict__ r, const lon
   for (long long c = beg + threadIdx.x; c < end; c += blockDim.x) {
     const double v = r[c];
     s += v * v;
-    mx = fmax(mx, fabs(v));
+    mx = max_keep_nan(mx, fabs(v));
   }
   __shared__ double ss[256], sm[256];
   ss[threadIdx.x] = s;
@@ -99,7 +103,7 @@ __global__ void residual_partials_kernel(const double* __restrict__ r, const lon
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) {
       ss[threadIdx.x] += ss[threadIdx.x + w];
-      sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+      sm[threadIdx.x] = max_keep_nan(sm[threadIdx.x], sm[threadIdx.x + w]);
     }
     __syncthreads();
   }
@@ -117,7 +121,7 @@ __global__ void residual_finalize_kernel(const double* __restrict__ part, const 
   double s = 0.0, mx = 0.0;
   for (int b = case_chunk0[cs]; b < case_chunk0[cs + 1]; b++) {
     s += part[2 * b];
-    mx = fmax(mx, part[2 * b + 1]);
+    mx = max_keep_nan(mx, part[2 * b + 1]);
   }
   const long long n = case_cells[cs];
   out[2 * cs] = n > 0 ? sqrt(s / double(n)) : 0.0;
@@ -153,6 +157,27 @@ void set_last_error_text(const std::string& msg) { g_create_error = msg; }
 // Largest cell count one solver takes: 20 rows of (N rounded up to 64) int
 // offsets must stay below 2^31 (107,374,080 cells).
 constexpr int64_t kMaxCells = (int64_t(INT32_MAX) / 20) / 64 * 64 - 64;
+static_assert(20 * ((kMaxCells + 63) / 64 * 64) <= int64_t(INT32_MAX), "face-state rows of the largest mesh");
+
+extern "C" int nf_check_mesh_size(int64_t n_cells, int64_t n_faces) {
+  if (n_cells <= 0 || n_faces < 0) {
+    g_create_error = "mesh has no cells";
+    return NF_ERR_MESH;
+  }
+  // The stage kernels index the 20 face-state rows of [20][stride] arrays
+  // with 32-bit products, so 20 * stride must stay below 2^31; faces are
+  // numbered in 32-bit ints as well.
+  if (n_cells > kMaxCells) {
+    g_create_error = "mesh too large for one solver: " + std::to_string(n_cells) + " cells, at most " +
+                     std::to_string(kMaxCells) + " (split larger meshes across solvers)";
+    return NF_ERR_MESH;
+  }
+  if (n_faces >= (int64_t(1) << 30)) {
+    g_create_error = "mesh too large for one solver: " + std::to_string(n_faces) + " faces, at most 2^30 - 1";
+    return NF_ERR_MESH;
+  }
+  return NF_OK;
+}
 
 struct nf_solver {
   int device = 0;
@@ -786,12 +811,7 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     cudaStream_t st = s->stream;
 
     const int64_t N = m.n_cells, F = m.n_faces;
-    if (N >= (int64_t(1) << 30) || F >= (int64_t(1) << 30)) throw std::runtime_error("mesh too large for one solver");
-    // The stage kernels index the 20 face-state rows of [20][stride] arrays
-    // with 32-bit products, so 20 * stride must stay below 2^31.
-    if (N > kMaxCells)
-      throw std::runtime_error("mesh too large for one solver: at most " + std::to_string(kMaxCells) +
-                               " cells (split larger meshes across solvers)");
+    if (nf_check_mesh_size(N, F) != NF_OK) throw std::runtime_error(g_create_error);
     s->n = int(N);
     s->stride = int((N + 63) / 64 * 64);
     s->n_faces = int(F);

@@ -6,7 +6,7 @@ reference solver compiled from its own unmodified sources, on small seeded
 meshes from netflux_b200.meshgen. Machines without the reference tree read
 these files instead.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]   # all cases when none is named
 
 Each ``<case>.npz`` holds the mesh (nodes, tets as written, markers), the
 initial state, the free stream, and the reference's outputs:
@@ -45,6 +45,15 @@ CASES = {
                                                                 ("imin", "imax", "jmin", "jmax", "kmin", "kmax")},
                                                   patch_types={"walls": mg.SLIP_WALL}),
                      fs=(1.0, 0.3, -0.2, 0.1, 1.0), U0=mg.cube_initial_state, steps100=True),
+    # box with every boundary type: no-slip walls (BC_NoSlipWall, Numerics.cpp:59-66) at z = 0 and 1,
+    # slip walls at y = 0 and 1, far field at x = 0 and 1
+    "wallbox5": dict(mesh=lambda: mg.box_tet_mesh(5, 5, 5, jitter=0.1, seed=14,
+                                                  side_patches={"imin": "farfield", "imax": "farfield",
+                                                                "jmin": "slip", "jmax": "slip",
+                                                                "kmin": "noslip", "kmax": "noslip"},
+                                                  patch_types={"farfield": mg.FAR_FIELD, "slip": mg.SLIP_WALL,
+                                                               "noslip": mg.NO_SLIP_WALL}),
+                     fs=(1.0, 0.4, 0.1, -0.2, 1.0 / 1.4), U0=mg.cube_initial_state, steps100=True),
 }
 
 
@@ -94,9 +103,13 @@ def make(name: str, spec: dict, tmp: str) -> None:
 def main() -> None:
     if not po.reference_available():
         raise SystemExit("oracle/_ref/nf_ref_nodump is not built (make -C oracle with the reference tree present)")
+    names = sys.argv[1:] or list(CASES)
+    unknown = [n for n in names if n not in CASES]
+    if unknown:
+        raise SystemExit(f"unknown case(s) {unknown}; known: {list(CASES)}")
     with tempfile.TemporaryDirectory() as tmp:
-        for name, spec in CASES.items():
-            make(name, spec, tmp)
+        for name in names:
+            make(name, CASES[name], tmp)
 
 
 if __name__ == "__main__":

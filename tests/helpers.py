@@ -11,7 +11,7 @@ from netflux_b200 import meshgen as mg
 from netflux_b200 import solver as S
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ("cube4", "sod40", "bump12", "slipbox5")
+CASES = ("cube4", "sod40", "bump12", "slipbox5", "wallbox5")
 
 
 @lru_cache(maxsize=None)
@@ -54,6 +54,32 @@ def rel_linf(a: np.ndarray, b: np.ndarray) -> float:
 
 def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+VARIABLES = ("rho", "rho_u", "rho_v", "rho_w", "E")
+
+
+def per_variable(a: np.ndarray, b: np.ndarray) -> Dict[str, Dict[str, float]]:
+    """Errors of each conserved variable on its own: relative L-infinity
+    max|a_k - b_k| / max|b_k| and relative L2 ||a_k - b_k|| / ||b_k||, plus the
+    absolute L-infinity. Unlike rel_linf, every momentum component is measured
+    against its own scale, so a component that is nearly zero everywhere shows
+    a large relative figure for round-off-sized absolute differences."""
+    a = np.asarray(a).reshape(b.shape[0], -1)
+    b = np.asarray(b).reshape(b.shape[0], -1)
+    out = {}
+    for k, name in enumerate(VARIABLES[: b.shape[1]]):
+        d = a[:, k] - b[:, k]
+        out[name] = {"rel_linf": float(np.abs(d).max() / max(np.abs(b[:, k]).max(), 1e-300)),
+                     "rel_l2": float(np.linalg.norm(d) / max(np.linalg.norm(b[:, k]), 1e-300)),
+                     "abs_linf": float(np.abs(d).max()),
+                     "scale": float(np.abs(b[:, k]).max())}
+    return out
+
+
+def format_per_variable(errs: Dict[str, Dict[str, float]]) -> str:
+    return "; ".join(f"{n}: Linf {e['rel_linf']:.2e} L2 {e['rel_l2']:.2e} (abs {e['abs_linf']:.1e}, "
+                     f"scale {e['scale']:.1e})" for n, e in errs.items())
 
 
 def gpu_available() -> bool:

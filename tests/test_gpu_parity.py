@@ -286,6 +286,20 @@ def test_nonphysical_state_is_reported():
         s.synchronize()
 
 
+def test_residual_max_norm_keeps_nan():
+    """A NaN in the state makes both residual norms NaN: the max norm does not drop it."""
+    g = golden("cube4")
+    U0 = g["U0"].copy()
+    U0[17, 1] = np.nan
+    cfg = config_for(precision="fp64", freestream=tuple(g["freestream"]))
+    s = S.EulerSolver(cfg, mesh(g), U0=U0)
+    s.calc_timestep(cfg)
+    s.step(cfg)
+    r = s.residual()
+    assert np.isnan(r[0, 0]) and np.isnan(r[0, 1]), r
+    s.close()
+
+
 def test_sod_tube_against_oracle_and_mixed_error():
     """Sod tube with the limiter active at the shock: FP64 and mixed vs the oracle."""
     m = mg.sod_mesh(100, 4, 4, jitter=0.05, seed=5)

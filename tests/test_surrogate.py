@@ -100,7 +100,7 @@ def test_warm_start_gains_over_free_stream_start():
     assert plain["converged"] and warm["converged"] and warm["fallback"] is None
     assert warm["res_final"] <= 1e-6 * plain["res_fs"]
     assert warm["steps"] < plain["steps"]
-    assert d <= 1e-5
+    assert d <= 1e-6  # the warm-started solve lands within 1e-6 relative L2 of the plain one
 
 
 def test_wall_distance_matches_brute_force():

@@ -66,3 +66,19 @@ def test_residual_norms_noalloc_rejects_oversize_and_handles_empty():
     assert _call(empty, out, stream) == L.NF_OK
     torch.cuda.synchronize()
     assert out.cpu().numpy().tolist() == [0.0, 0.0]
+
+
+def test_residual_norms_noalloc_keeps_nan():
+    """A NaN anywhere in the values shows in both norms (a non-finite residual must not vanish from
+    the max norm), in the first block and in a later one."""
+    import torch
+
+    stream = torch.cuda.current_stream().cuda_stream
+    out = torch.full((2,), -1.0, dtype=torch.float64, device="cuda")
+    for pos in (5, 40000):
+        v = torch.linspace(-1.0, 1.0, 50000, dtype=torch.float64, device="cuda")
+        v[pos] = float("nan")
+        assert _call(v, out, stream) == L.NF_OK, L.last_error(None)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert np.isnan(got[0]) and np.isnan(got[1]), (pos, got)
