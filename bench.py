@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--scale", type=int, default=1, help="divide the hex counts (quick runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--steady", action="store_true",
                     help="also time a local-time-stepping solve to a 1e-6 density-residual drop")
     ap.add_argument("--steady-max", type=int, default=60000)
@@ -84,6 +84,12 @@ def case_mesh(name: str, scale: int):
         return m, fs, mg.cube_initial_state(m), False, "unit cube 20^3 hexes, 6 tets each, Gaussian density bump"
     m = mg.sod_mesh(400 // scale, 8, 8, jitter=0.05, seed=4321)
     return m, mg.SOD_LEFT, mg.sod_initial_state(m), False, "Sod tube 400x8x8 hexes, 6 tets each"
+
+
+def case_mesh_desc(name: str) -> str:
+    return {"bump": "bump channel 128x64x64 hexes, 6 tets each",
+            "cube": "unit cube 20^3 hexes, 6 tets each, Gaussian density bump",
+            "sod": "Sod tube 400x8x8 hexes, 6 tets each"}[name]
 
 
 def measured_peaks():
@@ -156,12 +162,14 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
                       local_dt: bool):
     """Compulsory HBM bytes of one launch of each stage kernel (every datum the
     kernel must read or write, once; neighbours' values are other cells' own
-    values and are not counted again).
+    values and are not counted again), averaged over the three stages.
 
     FP64 (gradient_node / flux_node), per cell:
       gradient: V (40), 4 vertex ids (16), 4 neighbour ids (16), face code (4),
         vol (8), writes 4 face states (160); per node 32 (xyz + pad); per
-        boundary face one ghost state (40).
+        boundary face one ghost state (40); the last stage also reads dS (24)
+        and writes the next step's dt (8 with local time stepping): a third of
+        that on average.
       flux: 4 own face states (160), 4 neighbour face ids (16), face code (4),
         4 vertex ids (16), U (40), U^n (40 at stages 2 and 3: 2/3 on average),
         vol (8), local dt (8 with local time stepping), writes U and V (80) and
@@ -180,7 +188,7 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
         grad = n_cells * (40 + 16 + 16 + 4 + 8 + 80) + n_nodes * 16 + n_boundary * 40
         flux = n_cells * (40 + 80 + 16 + 4 + 16 + upd) + n_nodes * 16 + n_boundary * 20
     else:
-        grad = n_cells * (40 + 16 + 16 + 4 + 8 + 160) + n_nodes * 32 + n_boundary * 40
+        grad = n_cells * (40 + 16 + 16 + 4 + 8 + 160 + (24 + lts) / 3) + n_nodes * 32 + n_boundary * 40
         flux = n_cells * (160 + 16 + 4 + 16 + upd) + n_nodes * 32 + n_boundary * 40
     return {"flux": flux, "gradient": grad}
 
@@ -203,17 +211,34 @@ def model_bytes_per_cell_stage(n_cells: int, n_faces: int) -> float:
     return step / (3.0 * n_cells)
 
 
-def cpu_reference_baseline(n_steps: int = 3, case: str = "bump", scale: int = 2, procs: int = 0):
+# host memory one reference process holds per cell (2.36 GB at 3,145,728 tets), with a margin
+REF_BYTES_PER_CELL = 1000.0
+
+
+def host_processes(n_cells: int) -> int:
+    """Independent reference processes to run at once: one per host core, at most as many as the
+    available host memory holds."""
+    n = os.cpu_count() or 1
+    try:
+        with open("/proc/meminfo") as f:
+            avail = next(int(l.split()[1]) * 1024 for l in f if l.startswith("MemAvailable:"))
+        n = max(1, min(n, int(0.8 * avail // (REF_BYTES_PER_CELL * n_cells))))
+    except Exception:
+        pass
+    return n
+
+
+def cpu_reference_baseline(n_steps: int = 3, case: str = "bump", scale: int = 1, procs: int = 0):
     """Time the compiled reference on a bounded sample of a workload: the case's
-    mesh (the bump channel at half resolution by default), n_steps TVD-RK3
-    steps per single-threaded process."""
+    full mesh (scale 1), n_steps TVD-RK3 steps per single-threaded process, the
+    solve timed inside each process (mesh reading and building excluded)."""
     from netflux_b200 import meshgen as mg
     from oracle import pyoracle as po  # CPU baseline leg only
     variant = "nf_ref_nodump"
     if not po.reference_available(variant):
         return None
     m, fs, U0, _, desc = case_mesh(case, scale)
-    nproc = procs or (os.cpu_count() or 1)
+    nproc = procs or host_processes(m.n_cells)
     with tempfile.TemporaryDirectory() as tmp:
         case_dir = os.path.join(tmp, "case")
         mg.write_case(case_dir, m, fs, U0=U0)
@@ -243,9 +268,10 @@ def cpu_reference_baseline(n_steps: int = 3, case: str = "bump", scale: int = 2,
         "single_core": cs / one / 1e6,
         "all_cores": cs * len(many) / max(many) / 1e6,
         "cores": nproc,
-        "sample": f"{desc} (hex counts / {scale}: {m.n_cells} tets), {n_steps} TVD-RK3 steps per process, "
-                  f"reference compiled from its sources (debug dump linked out), {nproc} independent "
-                  f"single-threaded processes",
+        "sample": f"{desc} ({m.n_cells} tets{', hex counts / %d' % scale if scale > 1 else ', the full mesh'}), "
+                  f"{n_steps} TVD-RK3 steps per process, reference compiled from its sources (debug dump "
+                  f"linked out), {nproc} independent single-threaded processes, solve time only",
+        "same_config": scale == 1,
     }
 
 
@@ -257,20 +283,60 @@ def run_reference_arm(args):
     if not po.reference_available("nf_ref_nodump"):
         print(json.dumps({"impl": "reference", "unavailable": "reference build (oracle/_ref) missing"}))
         return
-    nproc = os.cpu_count() or 1
-    scale = args.scale if args.case != "bump" else max(2, args.scale)  # the bump sample: half resolution
-    res = cpu_reference_baseline(n_steps=max(1, args.steps), case=args.case, scale=scale, procs=nproc)
+    # every step of every process is one TVD-RK3 step of the full workload; the sample is bounded
+    # to 3 steps per process at the 3.1M-tet channel (about 10 s of solving each)
+    n_steps = max(1, min(args.steps, 3 if args.case == "bump" and args.scale == 1 else args.steps))
+    res = cpu_reference_baseline(n_steps=n_steps, case=args.case, scale=args.scale)
     val = res["all_cores"]
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(val, 3), "unit": "Mcell-stages/s",
         "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.case}, TVD-RK3 FP64 (bounded sample)", "sample": res["sample"]},
+        "config": {"workload": case_mesh_desc(args.case), "sample": res["sample"],
+                   "same_config": res["same_config"]},
         "cpu_baseline": {"value": round(val, 3), "unit": "Mcell-stages/s", "cores": res["cores"],
                          "kind": "reference", "sample": res["sample"],
-                         "single_core": round(res["single_core"], 4)},
+                         "single_core": round(res["single_core"], 4), "same_config": res["same_config"]},
         "e2e": {"value": round(val, 3), "unit": "Mcell-stages/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def host_link(nbytes: int, reps: int = 5):
+    """Pinned host <-> device copy rates (GB/s) for one transfer of nbytes: host to device alone,
+    device to host alone, and both at once on two streams (the total of both directions), each over
+    reps back-to-back copies timed with CUDA events on the copying streams."""
+    import torch
+    n = nbytes // 8
+    h_in = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    h_out = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    d_a = torch.empty(n, dtype=torch.float64, device="cuda")
+    d_b = torch.empty(n, dtype=torch.float64, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def run(h2d: bool, d2h: bool) -> float:
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        start.record()
+        ends = []
+        for on, st, fn in ((h2d, s1, lambda: d_a.copy_(h_in, non_blocking=True)),
+                           (d2h, s2, lambda: h_out.copy_(d_b, non_blocking=True))):
+            if not on:
+                continue
+            st.wait_event(start)
+            with torch.cuda.stream(st):
+                for _ in range(reps):
+                    fn()
+                e = torch.cuda.Event(enable_timing=True)
+                e.record()
+            ends.append(e)
+        torch.cuda.synchronize()
+        return max(start.elapsed_time(e) for e in ends) / 1e3
+
+    run(True, True)  # warm
+    t_in, t_out, t_both = run(True, False), run(False, True), run(True, True)
+    return {"bytes": int(nbytes), "h2d_gbs": round(reps * nbytes / t_in / 1e9, 2),
+            "d2h_gbs": round(reps * nbytes / t_out / 1e9, 2),
+            "both_total_gbs": round(2 * reps * nbytes / t_both / 1e9, 2)}
 
 
 def main():
@@ -382,6 +448,7 @@ def main():
                 solver.step(cfg)
                 solver.snapshot_begin(outs[i % 2])
             solver.snapshot_wait()
+            solver.upload_wait()
 
         def timed(loop):
             torch.cuda.synchronize()
@@ -398,9 +465,16 @@ def main():
         loop_streamed()
         v_sync = timed(loop_sync)
         v_stream = timed(loop_streamed)
+        link = host_link(N * 5 * 8)
+        # the copies' bound: each step moves one state in and one out, at the measured rate of
+        # both directions at once (or one direction alone, whichever bounds it more)
+        per_step_s = max(2 * N * 5 * 8 / (link["both_total_gbs"] * 1e9), N * 5 * 8 / (link["h2d_gbs"] * 1e9),
+                         N * 5 * 8 / (link["d2h_gbs"] * 1e9))
+        link["bound_value"] = round(N * 3 / per_step_s / 1e6, 3)
+        link["frac"] = round(v_stream / link["bound_value"], 4)
         e2e = {"value": round(v_stream, 3), "unit": "Mcell-stages/s",
                "h2d_bytes_per_step": int(N * 5 * 8), "d2h_bytes_per_step": int(N * 5 * 8 + 8),
-               "steps": n_e, "sync_value": round(v_sync, 3),
+               "steps": n_e, "sync_value": round(v_sync, 3), "host_link": link,
                "path": "per step, over the C ABI: upload_commit of a state copied from pinned memory, "
                        "calc_timestep, step, snapshot_begin into pinned memory; the next state's upload "
                        "and this result's copy run on side streams during the step, and the clock stops "
@@ -429,11 +503,12 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        # the same workload: the bump channel at half resolution, the small cases whole
-        res = cpu_reference_baseline(case=args.case, scale=max(2, args.scale) if args.case == "bump" else args.scale)
+        # the same workload and mesh
+        res = cpu_reference_baseline(case=args.case, scale=args.scale)
         if res is not None:
             cpu = {"value": round(res["all_cores"], 4), "unit": "Mcell-stages/s", "cores": res["cores"],
-                   "kind": "reference", "sample": res["sample"], "single_core": round(res["single_core"], 4)}
+                   "kind": "reference", "sample": res["sample"], "single_core": round(res["single_core"], 4),
+                   "same_config": res["same_config"]}
 
     if rank == 0:
         kernels_per_step = sum(kl) / max(args.steps // 2, 2)

@@ -195,27 +195,34 @@ int nf_get_state(nf_solver* s, double* U, int64_t n_cells);
  * the steps queued after this call, which do not change what is copied. U
  * must stay valid, and unread, until nf_snapshot_wait returns; with pinned
  * memory (cudaHostAlloc, cudaHostRegister) the copy is asynchronous, with
- * pageable memory the driver may complete it before returning. One snapshot
- * is in flight per solver: a second begin first waits for the first. Replaces
- * the synchronous solution read of Output::write_vtk_ascii (Output.cpp:17-45)
- * with one the step loop need not wait for. */
+ * pageable memory the driver may complete it before returning. Snapshots may
+ * overlap one another and the host never waits here: two device staging
+ * buffers are used in turn, and a gather waits on the device for the copy out
+ * of its buffer two snapshots back; the copies land in the order begun.
+ * Replaces the synchronous solution read of Output::write_vtk_ascii
+ * (Output.cpp:17-45) with one the step loop need not wait for. */
 int nf_snapshot_begin(nf_solver* s, double* U, int64_t n_cells);
-/* Wait until the snapshot started by nf_snapshot_begin is in host memory
- * (NF_OK at once when none is in flight). */
+/* Wait until every snapshot begun so far is in host memory (NF_OK at once
+ * when none is in flight). */
 int nf_snapshot_wait(nf_solver* s);
 /* The other direction: start copying a conserved state (reference cell
  * order, [n_cells][5]) from host memory U to the device on a side stream,
  * overlapping the work already queued, which it does not change; U must stay
- * valid and unchanged until nf_upload_commit returns (pinned memory makes the
- * copy asynchronous). One upload in flight per solver: a second begin before
- * the commit is NF_ERR_ARG. nf_upload_commit then makes that state the
- * solver's state exactly as nf_set_state does, queued after the work already
- * queued, and returns once the copy has landed; NF_ERR_ARG without a begin.
+ * valid and unchanged until nf_upload_wait returns (pinned memory makes the
+ * copy asynchronous). One upload per solver between begin and commit: a
+ * second begin before the commit is NF_ERR_ARG. nf_upload_commit then makes
+ * that state the solver's state exactly as nf_set_state does, queued on the
+ * device after the work already queued and after the copy, and returns
+ * without waiting; NF_ERR_ARG without a begin. The next begin may follow at
+ * once (its copy waits on the device until the committed state has been
+ * taken from the staging buffer). nf_upload_wait blocks until the last
+ * upload's copy has landed, after which its host buffer may change.
  * Together with the snapshots this streams independent states through one
- * solver with both copies overlapping the steps. No counterpart in the
- * reference (it has no device memory). */
+ * solver with both copies overlapping the steps and the host never waiting
+ * on a copy. No counterpart in the reference (it has no device memory). */
 int nf_upload_begin(nf_solver* s, const double* U, int64_t n_cells);
 int nf_upload_commit(nf_solver* s);
+int nf_upload_wait(nf_solver* s);
 /* U^n of the next step's TVD-RK3 combination (the reference's solution_old,
  * Solver.cpp:127-132), AoS [n_cells][5] in reference cell order; applies to
  * the next step only (afterwards U^n is the state, Solver.cpp:51).

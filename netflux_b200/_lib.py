@@ -30,7 +30,7 @@ EXPORTED = (
     "nf_mesh_export", "nf_mesh_get_permutation", "nf_mesh_get_case_offsets", "nf_mesh_destroy",
     "nf_params_default", "nf_create", "nf_set_state", "nf_get_state", "nf_set_state_old", "nf_calc_timestep", "nf_set_timestep",
     "nf_step", "nf_advance", "nf_get_residual", "nf_get_field", "nf_synchronize", "nf_last_error", "nf_destroy",
-    "nf_time_steps", "nf_residual_norms_noalloc", "nf_tune", "nf_set_launch_shapes", "nf_snapshot_begin", "nf_snapshot_wait", "nf_upload_begin", "nf_upload_commit", "nf_solve_steady", "nf_solve_steady_to", "nf_fastmath_selftest", "nf_check_mesh_size", "nf_set_host_threads",
+    "nf_time_steps", "nf_residual_norms_noalloc", "nf_tune", "nf_set_launch_shapes", "nf_snapshot_begin", "nf_snapshot_wait", "nf_upload_begin", "nf_upload_commit", "nf_upload_wait", "nf_solve_steady", "nf_solve_steady_to", "nf_fastmath_selftest", "nf_check_mesh_size", "nf_set_host_threads",
     "nf_mlp_param_count", "nf_mlp_create", "nf_mlp_last_error", "nf_mlp_destroy", "nf_mlp_get_params",
     "nf_mlp_set_params", "nf_mlp_set_data", "nf_mlp_train", "nf_mlp_gradients", "nf_mlp_predict",
     "nf_mlp_gemm_selftest", "nf_wall_distance",
@@ -112,6 +112,7 @@ def load() -> C.CDLL:
         "nf_snapshot_wait": (I, [P]),
         "nf_upload_begin": (I, [P, C.POINTER(C.c_double), C.c_int64]),
         "nf_upload_commit": (I, [P]),
+        "nf_upload_wait": (I, [P]),
         "nf_solve_steady": (I, [P, D, I64, I, i64p, dp, dp, dp]),
         "nf_solve_steady_to": (I, [P, dp, I64, I, i64p, dp, dp, dp]),
         "nf_fastmath_selftest": (I, [dp, I64, dp, dp]),

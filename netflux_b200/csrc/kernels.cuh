@@ -106,6 +106,15 @@ struct StageArgs {
   float* phi_keep32;
 };
 
+// Programmatic dependent launch (the fast forms' stage kernels are launched
+// with programmatic stream serialization, solver.cu): a kernel lets the next
+// one in the stream launch once all of its blocks have started, and waits for
+// the previous one to complete (its writes visible) before reading anything
+// that kernel wrote. The next kernel's launch and block set-up then overlap
+// this one's last wave. Launched without the attribute, both are no-ops.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
+__device__ __forceinline__ void pdl_wait_previous() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Once a case's ratchet is on, a cell's limiter value is the minimum of the
 // live value and the kept one, and is kept: it only tightens, so it settles
 // and the steady residual can converge (the live Barth limiter makes it stall).
@@ -125,7 +134,9 @@ __device__ __forceinline__ T ratchet(const StageArgs& a, size_t at, T phi) {
   return v;
 }
 
-enum : int { kScalDtMin = 0, kScalTime = 1, kScalTEnd = 2, kScalDtUsed = 3, kScalCount = 8 };
+// device scalars: the step's dt (minimum), the time, t_end, the dt last used,
+// and the next step's dt while the last stage computes it
+enum : int { kScalDtMin = 0, kScalTime = 1, kScalTEnd = 2, kScalDtUsed = 3, kScalDtNext = 4, kScalCount = 8 };
 
 __device__ __forceinline__ double stage_dt(const double* scal) {
   double dt = scal[kScalDtMin];
@@ -406,6 +417,45 @@ __global__ void __launch_bounds__(256) flux_update_kernel(MeshView<T> m, StageAr
   }
 }
 
+// Per-cell CFL time step of EulerSolver::calc_timestep (Solver.cpp:232-274) on
+// one cell's primitives, every operation rounded on its own (no contraction)
+// in the reference's order, so the result is the reference's bit for bit in
+// every translation unit.
+__device__ __forceinline__ double dt_of_cell(const double V[5], double dS0, double dS1, double dS2, double vol,
+                                             double cfl) {
+  const double cs = __dsqrt_rn(__ddiv_rn(__dmul_rn(Gas<double>::gamma, V[4]), V[0]));
+  const double sx = __dmul_rn(__dadd_rn(fabs(V[1]), cs), dS0);
+  const double sy = __dmul_rn(__dadd_rn(fabs(V[2]), cs), dS1);
+  const double sz = __dmul_rn(__dadd_rn(fabs(V[3]), cs), dS2);
+  return __ddiv_rn(__dmul_rn(cfl, vol), __dadd_rn(__dadd_rn(sx, sy), sz));
+}
+
+// Minimum of v over the block, then one atomicMin on the bit pattern (exact
+// and order-free for positive doubles). Every thread of the block calls it.
+__device__ __forceinline__ void block_min_to(double v, unsigned long long* target) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, off));
+  __shared__ double wmin[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) wmin[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = (lane < int(blockDim.x + 31) / 32) ? wmin[lane] : DBL_MAX;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, off));
+    if (lane == 0 && v < DBL_MAX) atomicMin(target, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+// The next step's time step, computed by the FP64 form's last-stage gradient
+// kernel from the primitives it reads: those of the last stage input, which
+// the reference's calc_timestep reads (Solver.cpp:250).
+struct DtFuse {
+  double cfl;
+  double* dt_next;                  // per-cell dt of the next step (local time stepping) or null
+  unsigned long long* dt_min_bits;  // minimum over the cells (global time step)
+};
+
 // ---------------------------------------------------------------------------
 // Fast forms (FP64 with contraction, and mixed FP32): one thread per cell, the
 // cell's faces indexed by the vertex they face, geometry rebuilt from the
@@ -490,10 +540,9 @@ __device__ __forceinline__ void face_normals(const T P[4][3], T S[4][3]) {
 // together before any arithmetic (one exposed memory latency instead of five,
 // at the cost of registers); 3 as 0, with the cell's own rows prefetched
 // into L2 first.
-template <typename T, int kPipe, int kMinBlocks>
-__global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView<T> m, StageArgs a) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= m.n || frozen_cell(a, c)) return;
+// The body for one cell; vown receives the cell's own primitives.
+template <typename T, int kPipe>
+__device__ __forceinline__ void gradient_node_cell(const MeshView<T>& m, const StageArgs& a, int c, T vown[5]) {
   const int st = m.stride;
   static_assert(sizeof(T) == 8, "FP64 kernel");
   const T* __restrict__ Vin = a.Vin;
@@ -555,6 +604,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
   const T hv = T(0.5) * nr_rcp(T(m.vol[c]));
   const bool rat = a.barth && ratchet_on(a, c);
   auto variable = [&](int k, T vc, const T vo[4]) {
+    vown[k] = vc;
     T acc[3];
 #pragma unroll
     for (int e = 0; e < 3; e++) {
@@ -608,6 +658,47 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
       }
       variable(k, vc, vo);
     }
+  }
+}
+
+// CFL time step of one cell from its primitives with the fast forms'
+// reciprocal and reciprocal square root (within 2 ulp of dt_of_cell).
+__device__ __forceinline__ double dt_of_cell_fast(const double V[5], double dS0, double dS1, double dS2, double vol,
+                                                  double cfl) {
+  const double g = Gas<double>::gamma * V[4];
+  const double cs = g * nr_rsqrt(g * V[0]);  // sqrt(gamma p / rho)
+  const double sum = fma(fabs(V[3]) + cs, dS2, fma(fabs(V[2]) + cs, dS1, (fabs(V[1]) + cs) * dS0));
+  return cfl * vol * nr_rcp(sum);
+}
+
+// kDt: also the next step's time step from the cell's own primitives, after
+// the gradient work (the FP64 form's last stage; the primitives are those of
+// the last stage input, which the reference's calc_timestep reads,
+// Solver.cpp:250; every thread reaches the block minimum).
+template <typename T, int kPipe, int kMinBlocks, bool kDt = false>
+__global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView<T> m, StageArgs a, DtFuse dtf) {
+  static_assert(sizeof(T) == 8, "FP64 kernel");
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait_previous();
+  const bool in = c < m.n;
+  const bool active = in && !frozen_cell(a, c);
+  T vown[5];
+  if (active) gradient_node_cell<T, kPipe>(m, a, c, vown);
+  if constexpr (kDt) {
+    double dtc = DBL_MAX;
+    if (in) {
+      const int st = m.stride;
+      if (!active) {
+        if (dtf.dt_next) dtf.dt_next[c] = 0.0;  // a converged case keeps its state
+      } else {
+        const double d = dt_of_cell_fast(vown, m.dS[c], m.dS[st + c], m.dS[2 * st + c], m.vol[c], dtf.cfl);
+        if (dtf.dt_next) dtf.dt_next[c] = d;
+        if (!(d > 0.0) && !isnan(d)) atomicOr(a.status, kErrDt);
+        if (d > 0.0) dtc = d;  // std::min skips NaN (comparisons with NaN are false)
+      }
+    }
+    block_min_to(dtc, dtf.dt_min_bits);
   }
 }
 
@@ -668,6 +759,8 @@ __device__ __forceinline__ void stage_update(const StageArgs& a, int c, int st, 
 template <typename T, int kPipe, int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait_previous();
   if (c >= m.n || frozen_cell(a, c)) return;
   const int st = m.stride;
   const bool second = a.second_order != 0;
@@ -766,6 +859,8 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
 template <typename T, bool kRef>
 __global__ void __launch_bounds__(256) ghost_kernel(MeshView<T> m, StageArgs a) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait_previous();
   if (b >= m.nb) return;
   const int c = m.b_cell[b], f = m.b_face[b];
   const int F = m.n_faces, st = m.stride;
@@ -783,6 +878,8 @@ __global__ void __launch_bounds__(256) ghost_kernel(MeshView<T> m, StageArgs a) 
 template <typename T, bool kRef>
 __global__ void __launch_bounds__(256) boundary_flux_kernel(MeshView<T> m, StageArgs a) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait_previous();
   if (b >= m.nb) return;
   const int c = m.b_cell[b], q = m.b_fs[b], f = m.b_face[b];
   const int F = m.n_faces, st = m.stride;
@@ -832,12 +929,10 @@ __global__ void __launch_bounds__(256) timestep_kernel(MeshView<double> m, DtArg
   double dtc = DBL_MAX;
   if (c < m.n) {
     const int st = m.stride;
-    const double V0 = a.V[c], V1 = a.V[st + c], V2 = a.V[2 * st + c], V3 = a.V[3 * st + c], V4 = a.V[4 * st + c];
-    const double cs = sqrt(Gas<double>::gamma * V4 / V0);
-    const double sx = (fabs(V1) + cs) * m.dS[c];
-    const double sy = (fabs(V2) + cs) * m.dS[st + c];
-    const double sz = (fabs(V3) + cs) * m.dS[2 * st + c];
-    const double d = a.cfl * m.vol[c] / (sx + sy + sz);
+    double V[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) V[k] = a.V[k * st + c];
+    const double d = dt_of_cell(V, m.dS[c], m.dS[st + c], m.dS[2 * st + c], m.vol[c], a.cfl);
     const bool frozen = a.case_frozen && a.case_frozen[a.cell_case[c]];
     if (a.dt_local) a.dt_local[c] = frozen ? 0.0 : d;
     if (!frozen) {

@@ -1,6 +1,8 @@
 // Kernels with reciprocals and fused multiply-adds (FP64), and the
 // mixed-precision form (FP32 face work in difference variables, FP64 state,
 // primitives, ghosts, boundary fluxes and update).
+#include <utility>
+
 #include "kernels_mixed.cuh"
 #include "launch.hpp"
 
@@ -24,6 +26,24 @@ __global__ void __launch_bounds__(256) prim_kernel_fast(int n, int st, const dou
 
 static inline int grid_for(int n, int block) { return (n + block - 1) / block; }
 
+// Launch with programmatic stream serialization: the kernel may start while
+// the previous kernel in the stream finishes (it waits for it on the device
+// before reading its results, pdl_wait_previous). Captured into the step's
+// CUDA graph as a programmatic dependency.
+template <typename... P, typename... A>
+static void launch_pdl(void (*kernel)(P...), int grid, int block, cudaStream_t stream, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(grid));
+  cfg.blockDim = dim3(unsigned(block));
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
+
 // one thread per cell, at most 128 threads per block (the kernels' launch bounds)
 static inline int fast_block(int b) { return b > 128 ? 128 : b; }
 
@@ -45,22 +65,44 @@ constexpr int kCap3 = sizeof(T) == 8 ? 4 : 5;
     const int b = fast_block(l.block);                                                             \
     const int g = grid_for(m.n, b);                                                                \
     switch (l.variant) {                                                                            \
-      case 1: KERNEL<T, 1, 1><<<g, b, 0, l.stream>>>(m, a); break;                                 \
-      case 2: KERNEL<T, 0, kCap<T>><<<g, b, 0, l.stream>>>(m, a); break;                           \
-      case 3: KERNEL<T, 1, kCap<T>><<<g, b, 0, l.stream>>>(m, a); break;                           \
-      case 4: KERNEL<T, 0, kCap2<T>><<<g, b, 0, l.stream>>>(m, a); break;                          \
-      case 5: KERNEL<T, 1, kCap2<T>><<<g, b, 0, l.stream>>>(m, a); break;                          \
-      case 6: KERNEL<T, 2, 1><<<g, b, 0, l.stream>>>(m, a); break;                                 \
-      case 7: KERNEL<T, 2, kCap3<T>><<<g, b, 0, l.stream>>>(m, a); break;                          \
-      case 8: KERNEL<T, 3, kCap<T>><<<g, b, 0, l.stream>>>(m, a); break;                           \
-      case 9: KERNEL<T, 3, kCap2<T>><<<g, b, 0, l.stream>>>(m, a); break;                          \
-      default: KERNEL<T, 0, 1><<<g, b, 0, l.stream>>>(m, a); break;                                \
+      case 1: launch_pdl(KERNEL<T, 1, 1>, g, b, l.stream, m, a); break;                                 \
+      case 2: launch_pdl(KERNEL<T, 0, kCap<T>>, g, b, l.stream, m, a); break;                           \
+      case 3: launch_pdl(KERNEL<T, 1, kCap<T>>, g, b, l.stream, m, a); break;                           \
+      case 4: launch_pdl(KERNEL<T, 0, kCap2<T>>, g, b, l.stream, m, a); break;                          \
+      case 5: launch_pdl(KERNEL<T, 1, kCap2<T>>, g, b, l.stream, m, a); break;                          \
+      case 6: launch_pdl(KERNEL<T, 2, 1>, g, b, l.stream, m, a); break;                                 \
+      case 7: launch_pdl(KERNEL<T, 2, kCap3<T>>, g, b, l.stream, m, a); break;                          \
+      case 8: launch_pdl(KERNEL<T, 3, kCap<T>>, g, b, l.stream, m, a); break;                           \
+      case 9: launch_pdl(KERNEL<T, 3, kCap2<T>>, g, b, l.stream, m, a); break;                          \
+      default: launch_pdl(KERNEL<T, 0, 1>, g, b, l.stream, m, a); break;                                \
     }                                                                                               \
   } while (0)
 
-void launch_gradient_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
-  NF_NODE_DISPATCH(gradient_node_kernel, double, m, a, l);
+// the gradient kernel's variants, with and without the next step's time step
+#define NF_GRAD_DISPATCH(KDT)                                                                       \
+  do {                                                                                              \
+    const int b = fast_block(l.block);                                                             \
+    const int g = grid_for(m.n, b);                                                                \
+    switch (l.variant) {                                                                            \
+      case 1: launch_pdl(gradient_node_kernel<double, 1, 1, KDT>, g, b, l.stream, m, a, d); break;       \
+      case 2: launch_pdl(gradient_node_kernel<double, 0, kCap<double>, KDT>, g, b, l.stream, m, a, d); break; \
+      case 3: launch_pdl(gradient_node_kernel<double, 1, kCap<double>, KDT>, g, b, l.stream, m, a, d); break; \
+      case 4: launch_pdl(gradient_node_kernel<double, 0, kCap2<double>, KDT>, g, b, l.stream, m, a, d); break; \
+      case 5: launch_pdl(gradient_node_kernel<double, 1, kCap2<double>, KDT>, g, b, l.stream, m, a, d); break; \
+      case 6: launch_pdl(gradient_node_kernel<double, 2, 1, KDT>, g, b, l.stream, m, a, d); break;       \
+      case 7: launch_pdl(gradient_node_kernel<double, 2, kCap3<double>, KDT>, g, b, l.stream, m, a, d); break; \
+      case 8: launch_pdl(gradient_node_kernel<double, 3, kCap<double>, KDT>, g, b, l.stream, m, a, d); break; \
+      case 9: launch_pdl(gradient_node_kernel<double, 3, kCap2<double>, KDT>, g, b, l.stream, m, a, d); break; \
+      default: launch_pdl(gradient_node_kernel<double, 0, 1, KDT>, g, b, l.stream, m, a, d); break;      \
+    }                                                                                               \
+  } while (0)
+
+void launch_gradient_fast(const MeshView<double>& m, const StageArgs& a, const DtFuse* dt, Launch l) {
+  const DtFuse d = dt ? *dt : DtFuse{0.0, nullptr, nullptr};
+  if (dt) NF_GRAD_DISPATCH(true);
+  else NF_GRAD_DISPATCH(false);
 }
+#undef NF_GRAD_DISPATCH
 void launch_flux_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
   NF_NODE_DISPATCH(flux_node_kernel, double, m, a, l);
 }
@@ -70,16 +112,16 @@ void launch_flux_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
     const int b = fast_block(l.block);                                                             \
     const int g = grid_for(m.n, b);                                                                \
     switch (l.variant) {                                                                            \
-      case 1: KERNEL<1, 1><<<g, b, 0, l.stream>>>(m, a); break;                                    \
-      case 2: KERNEL<0, kCap<float>><<<g, b, 0, l.stream>>>(m, a); break;                          \
-      case 3: KERNEL<1, kCap<float>><<<g, b, 0, l.stream>>>(m, a); break;                          \
-      case 4: KERNEL<0, kCap2<float>><<<g, b, 0, l.stream>>>(m, a); break;                         \
-      case 5: KERNEL<1, kCap2<float>><<<g, b, 0, l.stream>>>(m, a); break;                         \
-      case 6: KERNEL<2, 1><<<g, b, 0, l.stream>>>(m, a); break;                                    \
-      case 7: KERNEL<2, kCap3<float>><<<g, b, 0, l.stream>>>(m, a); break;                         \
-      case 8: KERNEL<3, kCap<float>><<<g, b, 0, l.stream>>>(m, a); break;                          \
-      case 9: KERNEL<3, kCap2<float>><<<g, b, 0, l.stream>>>(m, a); break;                         \
-      default: KERNEL<0, 1><<<g, b, 0, l.stream>>>(m, a); break;                                   \
+      case 1: launch_pdl(KERNEL<1, 1>, g, b, l.stream, m, a); break;                                    \
+      case 2: launch_pdl(KERNEL<0, kCap<float>>, g, b, l.stream, m, a); break;                          \
+      case 3: launch_pdl(KERNEL<1, kCap<float>>, g, b, l.stream, m, a); break;                          \
+      case 4: launch_pdl(KERNEL<0, kCap2<float>>, g, b, l.stream, m, a); break;                         \
+      case 5: launch_pdl(KERNEL<1, kCap2<float>>, g, b, l.stream, m, a); break;                         \
+      case 6: launch_pdl(KERNEL<2, 1>, g, b, l.stream, m, a); break;                                    \
+      case 7: launch_pdl(KERNEL<2, kCap3<float>>, g, b, l.stream, m, a); break;                         \
+      case 8: launch_pdl(KERNEL<3, kCap<float>>, g, b, l.stream, m, a); break;                          \
+      case 9: launch_pdl(KERNEL<3, kCap2<float>>, g, b, l.stream, m, a); break;                         \
+      default: launch_pdl(KERNEL<0, 1>, g, b, l.stream, m, a); break;                                   \
     }                                                                                               \
   } while (0)
 
@@ -90,13 +132,13 @@ void launch_flux_mixed(const MeshView<float>& m, const StageArgs& a, Launch l) {
   NF_DELTA_DISPATCH(flux_delta_kernel, m, a, l);
 }
 void launch_ghost_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
-  if (m.nb > 0) ghost_kernel<double, false><<<grid_for(m.nb, l.block), l.block, 0, l.stream>>>(m, a);
+  if (m.nb > 0) launch_pdl(ghost_kernel<double, false>, grid_for(m.nb, l.block), l.block, l.stream, m, a);
 }
 void launch_bflux_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
-  if (m.nb > 0) boundary_flux_kernel<double, false><<<grid_for(m.nb, l.block), l.block, 0, l.stream>>>(m, a);
+  if (m.nb > 0) launch_pdl(boundary_flux_kernel<double, false>, grid_for(m.nb, l.block), l.block, l.stream, m, a);
 }
 void launch_bflux_mixed(const MeshView<double>& m, const StageArgs& a, Launch l) {
-  if (m.nb > 0) boundary_flux_delta_kernel<<<grid_for(m.nb, l.block), l.block, 0, l.stream>>>(m, a);
+  if (m.nb > 0) launch_pdl(boundary_flux_delta_kernel, grid_for(m.nb, l.block), l.block, l.stream, m, a);
 }
 __global__ void fastmath_kernel(const double* x, int n, double* rcp, double* rsq) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;

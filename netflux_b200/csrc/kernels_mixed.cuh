@@ -75,6 +75,8 @@ __device__ __forceinline__ void rusanov_delta(const float vc[5], const float dL[
 template <int kPipe, int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshView<float> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait_previous();
   if (c >= m.n || frozen_cell(a, c)) return;
   const int st = m.stride;
   const double* __restrict__ V = a.Vin;
@@ -205,6 +207,8 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshVie
 template <int kPipe, int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) flux_delta_kernel(MeshView<float> m, StageArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait_previous();
   if (c >= m.n || frozen_cell(a, c)) return;
   const int st = m.stride;
   const bool second = a.second_order != 0;
@@ -324,6 +328,8 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_delta_kernel(MeshView<fl
 // through the face; stored as FP32 difference.
 __global__ void __launch_bounds__(256) boundary_flux_delta_kernel(MeshView<double> m, StageArgs a) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait_previous();
   if (b >= m.nb) return;
   const int c = m.b_cell[b], q = m.b_fs[b], f = m.b_face[b];
   const int F = m.n_faces, st = m.stride;

@@ -24,7 +24,9 @@ void launch_timestep(const MeshView<double>& m, const DtArgs& a, Launch l);
 void launch_prim_ref(int n, int stride, const double* U, double* V, float* V32, Launch l);
 
 // fast FP64 and mixed FP32/FP64 (kernels_fast.cu)
-void launch_gradient_fast(const MeshView<double>& m, const StageArgs& a, Launch l);
+// dt, when not null, makes the gradient kernel compute the next step's time
+// step too (the last stage)
+void launch_gradient_fast(const MeshView<double>& m, const StageArgs& a, const DtFuse* dt, Launch l);
 void launch_flux_fast(const MeshView<double>& m, const StageArgs& a, Launch l);
 void launch_gradient_mixed(const MeshView<float>& m, const StageArgs& a, Launch l);
 void launch_flux_mixed(const MeshView<float>& m, const StageArgs& a, Launch l);

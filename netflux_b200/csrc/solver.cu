@@ -67,8 +67,9 @@ struct DevBuf {
 
 __global__ void scal_kernel(double* scal, int op, unsigned* status) {
   using namespace nf;
-  if (op == 0) {  // reset the dt minimum before the timestep kernel
+  if (op == 0) {  // reset the dt minima before the timestep kernel
     scal[kScalDtMin] = DBL_MAX;
+    scal[kScalDtNext] = DBL_MAX;
   } else {  // end of step: time += dt actually used
     // the computed dt must be valid (Solver.cpp:267-268); the dt clipped at
     // t_end may be 0 once the end time is reached
@@ -77,7 +78,20 @@ __global__ void scal_kernel(double* scal, int op, unsigned* status) {
     const double dt = stage_dt(scal);
     scal[kScalDtUsed] = dt;
     scal[kScalTime] = scal[kScalTime] + dt;
+    if (op == 2) {  // the last stage computed the next step's dt
+      scal[kScalDtMin] = scal[kScalDtNext];
+      scal[kScalDtNext] = DBL_MAX;
+    }
   }
+}
+
+// Copy the status word and the device scalars into host-mapped memory. The
+// host reads them after synchronising the solver stream; done by a kernel
+// rather than a device-to-host memcpy, so the read-back never queues on a
+// copy engine behind a large snapshot copy running on a side stream.
+__global__ void report_kernel(const unsigned* status, const double* scal, unsigned* h_status, double* h_scal) {
+  if (threadIdx.x == 0) *h_status = *status;
+  if (threadIdx.x < nf::kScalCount) h_scal[threadIdx.x] = scal[threadIdx.x];
 }
 
 // max(a, b) that keeps a NaN from either operand (fmax would drop it, and a
@@ -198,6 +212,12 @@ struct nf_solver {
   DevBuf<nf::PatchBC> patches;
   // state
   DevBuf<double> U, W, V0, V1, fs, grad, phi, R, dt_local, res_cell, scal, part, res_out, vg, fb;
+  // FP64 form: the last stage also computes the next step's dt, into the
+  // other per-cell dt buffer (dtl_cur names the one the next step uses);
+  // dt_ready says the next step's dt is already on the device
+  DevBuf<double> dt_local2;
+  int dtl_cur = 0;
+  bool dt_ready = false;
   DevBuf<double> Uold;       // U^n of the next step when set apart from U (nf_set_state_old)
   bool old_pending = false;
   DevBuf<float> fs32, grad32, phi32, fb32;  // mixed: increments, fields, boundary flux differences
@@ -215,6 +235,17 @@ struct nf_solver {
   std::vector<int> h_ratchet;
   int n_chunks = 0;
   double* h_scal = nullptr;  // pinned
+  // host-mapped copies of the status word and the scalars (report_kernel)
+  unsigned* h_rep_status = nullptr;
+  double* h_rep_scal = nullptr;
+  unsigned* d_rep_status = nullptr;
+  double* d_rep_scal = nullptr;
+  // status and scalars into the mapped buffers, then wait for the stream
+  void report() {
+    report_kernel<<<1, 32, 0, stream>>>(status.p, scal.p, d_rep_status, d_rep_scal);
+    ck(cudaGetLastError(), "report launch");
+    ck(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+  }
   int vcur = 0;              // V buffer holding the primitives of the current state
   bool stepped = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two steps from vcur = 0 / 1
@@ -228,9 +259,14 @@ struct nf_solver {
   DevBuf<double> stage;           // AoS staging for state transfers [N][5]
   // asynchronous state snapshots (nf_snapshot_begin / nf_snapshot_wait): a
   // second AoS staging buffer, copied to the host on its own stream
-  DevBuf<double> snap;
+  // Two staging buffers, used in turn: a snapshot's gather waits (on the
+  // device) only for the copy out of its buffer two snapshots back, so the
+  // host never blocks in nf_snapshot_begin.
+  DevBuf<double> snap[2];
   cudaStream_t snap_stream = nullptr;
-  cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
+  cudaEvent_t snap_ready = nullptr, snap_done[2] = {nullptr, nullptr};
+  bool snap_used[2] = {false, false};
+  int snap_k = 0;
   bool snap_pending = false;
   // asynchronous state uploads (nf_upload_begin / nf_upload_commit): a third
   // AoS staging buffer, filled from the host on its own stream
@@ -238,6 +274,7 @@ struct nf_solver {
   cudaStream_t up_stream = nullptr;
   cudaEvent_t up_done = nullptr, up_free = nullptr;  // copy landed; scatter done reading `up`
   bool up_pending = false, up_used = false;
+  bool up_reading = false;  // the last upload's copy may still read the caller's buffer
   DevBuf<long long> d_dev_of_ref;  // [N]
 
   // per-kernel timing: events around every launch while prof_on
@@ -265,6 +302,16 @@ struct nf_solver {
   }
 
   double* Vbuf(int i) { return i ? V1.p : V0.p; }
+  double* dtl(int i) { return i ? dt_local2.p : dt_local.p; }
+  // the FP64 form's last stage computes the next step's dt (second order:
+  // its gradient kernel reads the primitives the reference's dt reads)
+  bool fuse_dt() const {
+    return p.precision == NF_PREC_FP64 && p.spatial_order == NF_SECOND_ORDER && !p.dt_from_current_state;
+  }
+  void launch_prim(const double* Usrc, double* V) {
+    if (p.precision == NF_PREC_FP64_REF) nf::launch_prim_ref(n, stride, Usrc, V, nullptr, launch());
+    else nf::launch_prim_fast(n, stride, Usrc, V, nullptr, launch());
+  }
   nf::Launch launch() const { return nf::Launch{block, stream}; }
 
   nf::MeshView<double> view64() const {
@@ -280,6 +327,7 @@ struct nf_solver {
   }
 
   void enqueue_dt() {
+    if (dt_ready) return;  // the previous step's last stage computed it
     prof_begin(NF_KERNEL_OTHER);
     scal_kernel<<<1, 1, 0, stream>>>(scal.p, 0, status.p);
     prof_end();
@@ -287,7 +335,7 @@ struct nf_solver {
     const int vb = p.dt_from_current_state ? vcur : (stepped ? 1 - vcur : vcur);
     a.V = Vbuf(vb);
     a.cfl = p.cfl;
-    a.dt_local = p.local_time_stepping ? dt_local.p : nullptr;
+    a.dt_local = p.local_time_stepping ? dtl(dtl_cur) : nullptr;
     a.dt_min_bits = reinterpret_cast<unsigned long long*>(scal.p + nf::kScalDtMin);
     a.status = status.p;
     a.cell_case = cell_case.p;
@@ -299,10 +347,7 @@ struct nf_solver {
 
   // primitives of U in both V buffers (as after nf_set_state)
   void refresh_primitives() {
-    for (int b = 0; b < 2; b++) {
-      if (p.precision == NF_PREC_FP64_REF) nf::launch_prim_ref(n, stride, U.p, Vbuf(b), nullptr, launch());
-      else nf::launch_prim_fast(n, stride, U.p, Vbuf(b), nullptr, launch());
-    }
+    for (int b = 0; b < 2; b++) launch_prim(U.p, Vbuf(b));
   }
 
   void ratchet_reset() {
@@ -377,10 +422,10 @@ struct nf_solver {
     }
   }
 
-  void launch_gradient(const nf::StageArgs& a, const KCfg& k) {
+  void launch_gradient(const nf::StageArgs& a, const KCfg& k, const nf::DtFuse* dtf = nullptr) {
     const nf::Launch l{k.block, stream, k.variant};
     if (p.precision == NF_PREC_MIXED) nf::launch_gradient_mixed(view32(), a, l);
-    else if (p.precision == NF_PREC_FP64) nf::launch_gradient_fast(view64(), a, l);
+    else if (p.precision == NF_PREC_FP64) nf::launch_gradient_fast(view64(), a, dtf, l);
     else nf::launch_gradient_ref(view64(), a, launch());
   }
   void launch_flux(const nf::StageArgs& a, const KCfg& k) {
@@ -389,6 +434,9 @@ struct nf_solver {
     else if (p.precision == NF_PREC_FP64) nf::launch_flux_fast(view64(), a, l);
     else nf::launch_flux_ref(view64(), a, launch());
   }
+  // launch variants the tuner may pick (gradient, flux)
+  int grad_variants() const { return 10; }
+  int flux_variants() const { return 10; }
 
   // Arguments of the first stage of a step from the current state, writing
   // only scratch (face states, W, the other primitive buffer).
@@ -405,7 +453,7 @@ struct nf_solver {
     a.vg = vg.p;
     a.fb = fb.p;
     a.fb32 = fb32.p;
-    a.dt_local = dt_local.p;
+    a.dt_local = dtl(dtl_cur);
     a.scal = scal.p;
     a.status = status.p;
     a.Uin = U.p;
@@ -438,13 +486,16 @@ struct nf_solver {
       ck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
       return ms;
     };
-    const KCfg cands[] = {{128, 0}, {128, 1}, {128, 2}, {128, 3}, {128, 4}, {128, 5}, {128, 6},
-                          {128, 7}, {128, 8}, {128, 9}, {64, 0},  {64, 1},  {64, 2},  {64, 3},
-                          {64, 4},  {64, 5},  {64, 6},  {64, 7},  {64, 8},  {64, 9}};
+    auto cands = [](int n_variants) {
+      std::vector<KCfg> c;
+      for (int b : {128, 64})
+        for (int v = 0; v < n_variants; v++) c.push_back(KCfg{b, v});
+      return c;
+    };
     if (a.second_order) {
       nf::launch_ghost_fast(view64(), a, launch());
       float best = 1e30f;
-      for (const KCfg& k : cands) {
+      for (const KCfg& k : cands(grad_variants())) {
         const float t = time_it([&] { launch_gradient(a, k); });
         if (t < best) {
           best = t;
@@ -456,7 +507,7 @@ struct nf_solver {
     if (p.precision == NF_PREC_MIXED) nf::launch_bflux_mixed(view64(), a, launch());
     else nf::launch_bflux_fast(view64(), a, launch());
     float best = 1e30f;
-    for (const KCfg& k : cands) {
+    for (const KCfg& k : cands(flux_variants())) {
       const float t = time_it([&] { launch_flux(a, k); });
       if (t < best) {
         best = t;
@@ -478,6 +529,9 @@ struct nf_solver {
 
   void enqueue_step() {
     const int n_stages = p.time_scheme == NF_TVD_RK3 ? 3 : 1;
+    const bool fuse = fuse_dt();
+    nf::DtFuse dtf{p.cfl, p.local_time_stepping ? dtl(1 - dtl_cur) : nullptr,
+                   reinterpret_cast<unsigned long long*>(scal.p + nf::kScalDtNext)};
     for (int s = 0; s < n_stages; s++) {
       nf::StageArgs a{};
       a.second_order = p.spatial_order == NF_SECOND_ORDER;
@@ -498,7 +552,7 @@ struct nf_solver {
       a.phi = p.keep_stage_fields ? phi.p : nullptr;
       a.R = p.keep_stage_fields ? R.p : nullptr;
       a.res_cell = s == 0 ? res_cell.p : nullptr;
-      a.dt_local = dt_local.p;
+      a.dt_local = dtl(dtl_cur);
       a.scal = scal.p;
       a.status = status.p;
       if (ratchet_alloc) {
@@ -532,7 +586,7 @@ struct nf_solver {
         else nf::launch_ghost_fast(view64(), a, launch());
         prof_end();
         prof_begin(NF_KERNEL_GRADIENT);
-        launch_gradient(a, kgrad);
+        launch_gradient(a, kgrad, (fuse && s == n_stages - 1) ? &dtf : nullptr);
         prof_end();
       }
       prof_begin(NF_KERNEL_OTHER);
@@ -546,8 +600,12 @@ struct nf_solver {
       vcur = 1 - vcur;
     }
     prof_begin(NF_KERNEL_OTHER);
-    scal_kernel<<<1, 1, 0, stream>>>(scal.p, 1, status.p);
+    scal_kernel<<<1, 1, 0, stream>>>(scal.p, fuse ? 2 : 1, status.p);
     prof_end();
+    if (fuse) {
+      dtl_cur = 1 - dtl_cur;
+      dt_ready = true;
+    }
     stepped = true;
     old_pending = false;  // solution_old = solution (Solver.cpp:51)
   }
@@ -555,9 +613,8 @@ struct nf_solver {
   // Report a device-side failure as the reference would have (exceptions in
   // calc_timestep / check_flux_balance_validity become status codes).
   int check_status() {
-    unsigned st = 0;
-    ck(cudaMemcpyAsync(&st, status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream), "status D2H");
-    ck(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    report();
+    const unsigned st = *h_rep_status;
     if (st & nf::kErrNonFinite) {
       err = "unphysical values detected in the flux_balance field of the Euler solver (non-finite)";
       return NF_ERR_NONPHYSICAL;
@@ -580,11 +637,10 @@ struct nf_solver {
   void adopt_state(const double* aos) {
     const int st = stride;
     scatter_state_kernel<<<(n + 255) / 256, 256, 0, stream>>>(n, st, d_dev_of_ref.p, aos, U.p);
-    for (int b = 0; b < 2; b++) {
-      if (p.precision == NF_PREC_FP64_REF) nf::launch_prim_ref(n, st, U.p, Vbuf(b), nullptr, launch());
-      else nf::launch_prim_fast(n, st, U.p, Vbuf(b), nullptr, launch());
-    }
+    for (int b = 0; b < 2; b++) launch_prim(U.p, Vbuf(b));
     vcur = 0;
+    dtl_cur = 0;
+    dt_ready = false;
     stepped = false;
     old_pending = false;
     steps_done = 0;
@@ -593,11 +649,12 @@ struct nf_solver {
   }
 
   ~nf_solver() {
-    if (snap_pending) cudaEventSynchronize(snap_done);  // the copy still writes the caller's memory
+    if (snap_stream) cudaStreamSynchronize(snap_stream);  // copies may still write the caller's memory
     if (snap_ready) cudaEventDestroy(snap_ready);
-    if (snap_done) cudaEventDestroy(snap_done);
+    for (auto e : snap_done)
+      if (e) cudaEventDestroy(e);
     if (snap_stream) cudaStreamDestroy(snap_stream);
-    if (up_pending) cudaEventSynchronize(up_done);  // the copy still reads the caller's memory
+    if (up_pending || up_reading) cudaEventSynchronize(up_done);  // the copy still reads the caller's memory
     if (up_done) cudaEventDestroy(up_done);
     if (up_free) cudaEventDestroy(up_free);
     if (up_stream) cudaStreamDestroy(up_stream);
@@ -605,6 +662,8 @@ struct nf_solver {
       if (g) cudaGraphExecDestroy(g);
     for (auto e : prof_ev) cudaEventDestroy(e);
     if (h_scal) cudaFreeHost(h_scal);
+    if (h_rep_status) cudaFreeHost(h_rep_status);
+    if (h_rep_scal) cudaFreeHost(h_rep_scal);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -801,7 +860,8 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     s->block = p.block_size > 0 ? p.block_size : 256;
     if (p.block_size > 0) {
       s->kgrad.block = s->kflux.block = std::min(p.block_size, 128);
-      s->kgrad.variant = s->kflux.variant = std::max(0, std::min(p.kernel_variant, 9));
+      s->kgrad.variant = std::max(0, std::min(p.kernel_variant, s->grad_variants() - 1));
+      s->kflux.variant = std::max(0, std::min(p.kernel_variant, s->flux_variants() - 1));
       s->tuned = true;  // a caller-fixed shape is not tuned
     }
     if (s->block % 32 || s->block > 256) throw std::runtime_error("block_size must be a multiple of 32, <= 256");
@@ -999,11 +1059,11 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     s->b_patch.upload(hb_patch, st);
     s->rs.upload(h_rs, st);
     if (fast) {
-      s->cnode.upload(h_cnode, st);
       s->gcode.upload(h_gcode, st);
+      s->b_slotf.upload(hb_slotf, st);
+      s->cnode.upload(h_cnode, st);
       s->nbvf.upload(h_nbvf, st);
       s->nbsf.upload(h_nbsf, st);
-      s->b_slotf.upload(hb_slotf, st);
       std::vector<double> n4(size_t(4) * m.n_nodes, 0.0);
       for (int64_t v = 0; v < m.n_nodes; v++)
         for (int e = 0; e < 3; e++) n4[size_t(4 * v + e)] = m.nodes[size_t(3 * v + e)];
@@ -1055,6 +1115,8 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
       }
     }
     s->dt_local.alloc(static_cast<size_t>(stride));
+    s->dt_local2.alloc(static_cast<size_t>(stride));
+    s->dt_local2.zero(st);
     s->res_cell.alloc(static_cast<size_t>(stride));
     s->scal.alloc(nf::kScalCount);
     s->status.alloc(1);
@@ -1108,6 +1170,12 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     }
     s->res_out.alloc(size_t(2) * s->n_cases);
     ck(cudaMallocHost(&s->h_scal, nf::kScalCount * sizeof(double)), "cudaMallocHost");
+    ck(cudaHostAlloc(&s->h_rep_status, sizeof(unsigned), cudaHostAllocMapped), "cudaHostAlloc");
+    ck(cudaHostAlloc(&s->h_rep_scal, nf::kScalCount * sizeof(double), cudaHostAllocMapped), "cudaHostAlloc");
+    ck(cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_rep_status), s->h_rep_status, 0),
+       "cudaHostGetDevicePointer");
+    ck(cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->d_rep_scal), s->h_rep_scal, 0),
+       "cudaHostGetDevicePointer");
     std::fill(s->h_scal, s->h_scal + nf::kScalCount, 0.0);
     s->h_scal[nf::kScalTEnd] = p.t_end;
     ck(cudaMemcpyAsync(s->scal.p, s->h_scal, nf::kScalCount * sizeof(double), cudaMemcpyHostToDevice, st),
@@ -1176,25 +1244,28 @@ int nf_snapshot_begin(nf_solver* s, double* U, int64_t n_cells) {
       s->err = "nf_snapshot_begin: state size does not match the mesh";
       return NF_ERR_ARG;
     }
-    if (s->snap_pending) {  // one snapshot in flight per solver
-      ck(cudaEventSynchronize(s->snap_done), "snapshot wait");
-      s->snap_pending = false;
-    }
     if (!s->snap_stream) {
       ck(cudaStreamCreateWithFlags(&s->snap_stream, cudaStreamNonBlocking), "cudaStreamCreate");
       ck(cudaEventCreateWithFlags(&s->snap_ready, cudaEventDisableTiming), "cudaEventCreate");
-      ck(cudaEventCreateWithFlags(&s->snap_done, cudaEventDisableTiming), "cudaEventCreate");
+      for (auto& e : s->snap_done) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
     }
-    if (s->snap.n != size_t(5) * s->n) s->snap.alloc(size_t(5) * s->n);
+    const int k = s->snap_k;
+    if (s->snap[k].n != size_t(5) * s->n) s->snap[k].alloc(size_t(5) * s->n);
+    // the copy out of this staging buffer two snapshots back must be done
+    // before the gather overwrites it (a device-side wait, usually long met)
+    if (s->snap_used[k]) ck(cudaStreamWaitEvent(s->stream, s->snap_done[k], 0), "cudaStreamWaitEvent");
     // the gather is ordered after the queued steps and before the later ones
     gather_state_kernel<<<(s->n + 255) / 256, 256, 0, s->stream>>>(s->n, s->stride, s->d_dev_of_ref.p, s->U.p,
-                                                                   s->snap.p);
+                                                                   s->snap[k].p);
     ck(cudaGetLastError(), "snapshot gather");
     ck(cudaEventRecord(s->snap_ready, s->stream), "cudaEventRecord");
     ck(cudaStreamWaitEvent(s->snap_stream, s->snap_ready, 0), "cudaStreamWaitEvent");
-    ck(cudaMemcpyAsync(U, s->snap.p, size_t(5) * s->n * sizeof(double), cudaMemcpyDeviceToHost, s->snap_stream),
+    ck(cudaMemcpyAsync(U, s->snap[k].p, size_t(5) * s->n * sizeof(double), cudaMemcpyDeviceToHost,
+                       s->snap_stream),
        "snapshot D2H");
-    ck(cudaEventRecord(s->snap_done, s->snap_stream), "cudaEventRecord");
+    ck(cudaEventRecord(s->snap_done[k], s->snap_stream), "cudaEventRecord");
+    s->snap_used[k] = true;
+    s->snap_k = 1 - k;
     s->snap_pending = true;
     return NF_OK;
   });
@@ -1203,7 +1274,8 @@ int nf_snapshot_begin(nf_solver* s, double* U, int64_t n_cells) {
 int nf_snapshot_wait(nf_solver* s) {
   return guarded(s, [&]() -> int {
     if (!s->snap_pending) return NF_OK;
-    ck(cudaEventSynchronize(s->snap_done), "snapshot wait");
+    // the copies run in order on one stream: the last one done means all are
+    ck(cudaStreamSynchronize(s->snap_stream), "snapshot wait");
     s->snap_pending = false;
     return NF_OK;
   });
@@ -1248,8 +1320,16 @@ int nf_upload_commit(nf_solver* s) {
     ck(cudaGetLastError(), "nf_upload_commit");
     ck(cudaEventRecord(s->up_free, s->stream), "cudaEventRecord");
     s->up_used = true;
-    ck(cudaEventSynchronize(s->up_done), "upload wait");  // the caller's buffer is free again
     s->up_pending = false;
+    s->up_reading = true;  // until nf_upload_wait: the copy may still read the caller's buffer
+    return NF_OK;
+  });
+}
+
+int nf_upload_wait(nf_solver* s) {
+  return guarded(s, [&]() -> int {
+    if (s->up_pending || s->up_reading) ck(cudaEventSynchronize(s->up_done), "upload wait");
+    s->up_reading = false;
     return NF_OK;
   });
 }
@@ -1258,10 +1338,8 @@ int nf_calc_timestep(nf_solver* s, double* dt_out) {
   return guarded(s, [&]() -> int {
     s->enqueue_dt();
     ck(cudaGetLastError(), "timestep launch");
-    ck(cudaMemcpyAsync(s->h_scal, s->scal.p, nf::kScalCount * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
-       "scal D2H");
-    int rc = s->check_status();
-    const double dt = s->h_scal[nf::kScalDtMin];
+    int rc = s->check_status();  // also brings the scalars into h_rep_scal
+    const double dt = s->h_rep_scal[nf::kScalDtMin];
     if (dt_out) *dt_out = dt;
     if (rc == NF_OK && !(std::isfinite(dt) && dt > 0.0)) rc = NF_ERR_DT;
     if (rc == NF_ERR_DT) {
@@ -1304,10 +1382,7 @@ int nf_advance(nf_solver* s, int64_t n_steps, double* time_out) {
     s->run_steps(n_steps);
     ck(cudaGetLastError(), "advance launch");
     int rc = s->check_status();
-    if (time_out) {
-      ck(cudaMemcpy(s->h_scal, s->scal.p, nf::kScalCount * sizeof(double), cudaMemcpyDeviceToHost), "scal D2H");
-      *time_out = s->h_scal[nf::kScalTime];
-    }
+    if (time_out) *time_out = s->h_rep_scal[nf::kScalTime];
     return rc;
   });
 }
@@ -1476,7 +1551,7 @@ int nf_get_field(nf_solver* s, int which, double* out, int64_t n_values) {
       case NF_FIELD_GRADIENT: src = s->grad.p; comps = 15; break;
       case NF_FIELD_LIMITER: src = s->phi.p; break;
       case NF_FIELD_FLUX_BALANCE: src = s->R.p; break;
-      case NF_FIELD_LOCAL_DT: src = s->dt_local.p; comps = 1; break;
+      case NF_FIELD_LOCAL_DT: src = s->dtl(s->dtl_cur); comps = 1; break;
       default: s->err = "nf_get_field: unknown field"; return NF_ERR_ARG;
     }
     if (!src) {
@@ -1604,8 +1679,10 @@ int nf_set_launch_shapes(nf_solver* s, const int* config) {
     if (!config) return NF_ERR_ARG;
     for (int i = 0; i < 4; i += 2) {
       const int b = config[i], v = config[i + 1];
-      if (b < 32 || b > 128 || b % 32 || v < 0 || v > 9) {
-        s->err = "launch shapes: block must be 32..128 in steps of 32, variant 0..9";
+      const int nv = i == 0 ? s->grad_variants() : s->flux_variants();
+      if (b < 32 || b > 128 || b % 32 || v < 0 || v >= nv) {
+        s->err = "launch shapes: block must be 32..128 in steps of 32, variant 0.." + std::to_string(nv - 1) +
+                 (i == 0 ? " (gradient)" : " (flux)");
         return NF_ERR_ARG;
       }
     }

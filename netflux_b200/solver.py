@@ -33,6 +33,8 @@ SPATIAL_ORDERS = {"First": L.NF_FIRST_ORDER, "Second": L.NF_SECOND_ORDER}
 LIMITERS = {"NONE": L.NF_LIMITER_NONE, "Barth": L.NF_LIMITER_BARTH}
 PRECISIONS = {"fp64_ref": L.NF_PREC_FP64_REF, "fp64": L.NF_PREC_FP64, "mixed": L.NF_PREC_MIXED}
 STANDARD_AIR = (1.225, 0.0, 0.0, 0.0, 101325.0)  # Utilities.hpp:100-107
+# launch variants of the gradient and flux kernels each arithmetic form offers (the tuner's candidates)
+LAUNCH_VARIANTS = {"fp64_ref": (10, 10), "fp64": (10, 10), "mixed": (10, 10)}
 
 
 def _check(rc: int, handle=None) -> None:
@@ -381,15 +383,20 @@ class EulerSolver:
 
     def upload_begin(self, U: np.ndarray) -> None:
         """Start copying the state ``U`` (C-contiguous float64 [n_cells][5], reference order) to the
-        device while queued work runs; ``U`` must not change before upload_commit()."""
+        device while queued work runs; ``U`` must not change before upload_wait()."""
         if U.dtype != np.float64 or U.shape != (self.n_cells, 5) or not U.flags.c_contiguous:
             raise ValueError("upload buffer must be a C-contiguous float64 array of shape (n_cells, 5)")
         _check(L.load().nf_upload_begin(self._h, L.dptr(U), self.n_cells), self._h)
-        self._up = U  # kept alive while the copy runs
+        self._up = (getattr(self, "_up", None) or [])[-1:] + [U]  # kept alive while copies may run
 
     def upload_commit(self) -> None:
-        """Make the uploaded state the solver's state (as set_state does)."""
+        """Make the uploaded state the solver's state (as set_state does), queued on the device
+        after its copy; returns without waiting for the copy."""
         _check(L.load().nf_upload_commit(self._h), self._h)
+
+    def upload_wait(self) -> None:
+        """Wait until the last upload's copy has landed (its host buffer may change afterwards)."""
+        _check(L.load().nf_upload_wait(self._h), self._h)
         self._up = None
 
     def close(self):

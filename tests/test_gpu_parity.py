@@ -136,23 +136,28 @@ def test_every_launch_variant_computes_the_same_bits(precision):
     g = golden("bump12")
     cfg = config_for(precision=precision, freestream=tuple(g["freestream"]))
     out = {}
+    n_grad, n_flux = S.LAUNCH_VARIANTS[precision]
     for block in (64, 128):
-        for variant in range(10):
-            s = S.EulerSolver(cfg, mesh(g), U0=g["U0"], block_size=block, variant=variant)
-            s.advance(3)
-            out[(block, variant)] = s.get_solver_data().get_solution()
-            s.close()
+        for gv in range(n_grad):
+            for fv in range(n_flux) if gv == 0 else (0,):
+                s = S.EulerSolver(cfg, mesh(g), U0=g["U0"])
+                s.set_launch_shapes(gradient=(block, gv), flux=(block, fv))
+                s.advance(3)
+                out[(block, gv, fv)] = s.get_solver_data().get_solution()
+                s.close()
     # separate shapes for the two kernels, fixed through nf_set_launch_shapes
     s = S.EulerSolver(cfg, mesh(g), U0=g["U0"])
-    s.set_launch_shapes(gradient=(64, 7), flux=(128, 9))
+    s.set_launch_shapes(gradient=(64, n_grad - 1), flux=(128, n_flux - 1))
     s.advance(3)
     out["mixed shapes"] = s.get_solver_data().get_solution()
     with pytest.raises(L.NetFluxError):
-        s.set_launch_shapes(gradient=(64, 10), flux=(64, 0))
+        s.set_launch_shapes(gradient=(64, n_grad), flux=(64, 0))
+    with pytest.raises(L.NetFluxError):
+        s.set_launch_shapes(gradient=(64, 0), flux=(64, n_flux))
     with pytest.raises(L.NetFluxError):
         s.set_launch_shapes(gradient=(64, 0), flux=(200, 0))
     s.close()
-    ref = out[(128, 0)]
+    ref = out[(128, 0, 0)]
     for k, U in out.items():
         assert np.array_equal(U, ref), k
 

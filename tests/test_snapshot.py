@@ -41,7 +41,7 @@ def test_snapshot_holds_the_state_of_its_moment():
     assert L.load().nf_snapshot_begin(b._h, L.dptr(pageable), b.n_cells + 1) == L.NF_ERR_ARG
 
     b.snapshot_begin(pinned)
-    b.snapshot_begin(pageable)  # the second begin waits for the first
+    b.snapshot_begin(pageable)  # both in flight at once (two staging buffers), no host wait
     b.advance(2)
     assert np.array_equal(b.snapshot_wait(), ref7)
     b.snapshot_begin(pinned)
@@ -98,6 +98,7 @@ def test_upload_commit_equals_set_state_and_streams_with_snapshots():
         b.advance(1)
         b.snapshot_begin(outs[i % 2])  # this result's copy overlaps the next upload and step
     b.snapshot_wait()
+    b.upload_wait()  # the last input's copy has landed; its host buffer is free
     assert np.array_equal(outs[0], s1) and np.array_equal(outs[1], s1)
     b.upload_begin(ins[0])
     b.close()  # destroying the solver waits for the upload in flight
