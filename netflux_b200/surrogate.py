@@ -188,9 +188,15 @@ def case_features(mesh: S.Mesh, mach: float, h: float) -> np.ndarray:
 # ---------------------------------------------------------------------------
 # steady solves
 # ---------------------------------------------------------------------------
-def steady_config(fs: Sequence[float], precision: str = "mixed", limiter: str = "NONE") -> S.Config:
-    return S.Config(precision=precision, CFL=0.8, local_time_stepping=True, limiter=limiter, density_fs=fs[0],
-                    velocity_fs=list(fs[1:4]), pressure_fs=fs[4])
+# Limiter choices of the steady solves: the unlimited scheme (a reference option), or the
+# reference's Barth limiter with the limiter ratchet started once the residual has dropped 1e-2
+# (the live Barth limiter stalls the residual near a 2.5e-3..5e-3 drop).
+STEADY_LIMITERS = {"none": dict(limiter="NONE"), "barth-ratchet": dict(limiter="Barth", limiter_ratchet_drop=1e-2)}
+
+
+def steady_config(fs: Sequence[float], precision: str = "mixed", limiter: str = "none") -> S.Config:
+    return S.Config(precision=precision, CFL=0.8, local_time_stepping=True, density_fs=fs[0],
+                    velocity_fs=list(fs[1:4]), pressure_fs=fs[4], **STEADY_LIMITERS[limiter])
 
 
 def first_residual(solver: S.EulerSolver, U0: np.ndarray) -> float:
@@ -203,8 +209,8 @@ def first_residual(solver: S.EulerSolver, U0: np.ndarray) -> float:
 
 
 def solve_plain(mesh: S.Mesh, fs, tol: float = 1e-6, precision: str = "mixed", max_steps: int = 400000,
-                check_every: int = 100) -> dict:
-    cfg = steady_config(fs, precision)
+                check_every: int = 100, limiter: str = "none") -> dict:
+    cfg = steady_config(fs, precision, limiter)
     s = S.EulerSolver(cfg, mesh, U0=mg.uniform_state(mesh.n_cells, fs))
     s.tune()
     U_fs = mg.uniform_state(mesh.n_cells, fs)
@@ -217,7 +223,8 @@ def solve_plain(mesh: S.Mesh, fs, tol: float = 1e-6, precision: str = "mixed", m
 
 
 def solve_warm(mesh: S.Mesh, fs, mlp: MLP, mach: float, h: float, tol: float = 1e-6, precision: str = "mixed",
-               max_steps: int = 400000, check_every: int = 100, feats: Optional[np.ndarray] = None) -> dict:
+               max_steps: int = 400000, check_every: int = 100, feats: Optional[np.ndarray] = None,
+               limiter: str = "none") -> dict:
     """Warm-started steady solve with the free-stream fallback."""
     import time
     t0 = time.perf_counter()
@@ -225,7 +232,7 @@ def solve_warm(mesh: S.Mesh, fs, mlp: MLP, mach: float, h: float, tol: float = 1
     Y, ms_mlp = mlp.predict(f)
     U_w = denormalise_state(Y, fs)
     t_prep = time.perf_counter() - t0
-    cfg = steady_config(fs, precision)
+    cfg = steady_config(fs, precision, limiter)
     s = S.EulerSolver(cfg, mesh, U0=U_w)
     s.tune()
     U_fs = mg.uniform_state(mesh.n_cells, fs)

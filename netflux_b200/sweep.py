@@ -100,7 +100,7 @@ def build_case_meshes(cases: List[Dict], threads: int = 0) -> List[S.Mesh]:
 
 
 def run_batched(cases: List[Dict], precision: str = "mixed", tol: float = 1e-6, max_steps: int = 400000,
-                check_every: int = 100, device: int = -1) -> Dict:
+                check_every: int = 100, device: int = -1, limiter: str = "none") -> Dict:
     t0 = time.perf_counter()
     meshes = build_case_meshes(cases)
     fss = [mg.bump_freestream(c["mach"]) for c in cases]
@@ -108,7 +108,8 @@ def run_batched(cases: List[Dict], precision: str = "mixed", tol: float = 1e-6, 
     t_mesh = time.perf_counter() - t0
     states = [list(fs) for fs, m in zip(fss, meshes) for _ in m.patches()]
     U0 = np.concatenate([mg.uniform_state(m.n_cells, fs) for fs, m in zip(fss, meshes)])
-    s = S.EulerSolver(sur.steady_config(fss[0], precision), batch, U0=U0, patch_states=states, device=device)
+    s = S.EulerSolver(sur.steady_config(fss[0], precision, limiter), batch, U0=U0, patch_states=states,
+                      device=device)
     s.tune()
     out = s.solve_steady(tol, max_steps, check_every)
     U = s.get_solver_data().get_solution()
@@ -136,14 +137,16 @@ def training_data(res: Dict, cases: List[Dict]):
     return np.concatenate(F), np.concatenate(T)
 
 
-def evaluate(mlp: sur.MLP, pairs: List[Dict], nx: int, precision: str, tol: float, max_steps: int) -> List[Dict]:
+def evaluate(mlp: sur.MLP, pairs: List[Dict], nx: int, precision: str, tol: float, max_steps: int,
+             limiter: str = "none", check_every: int = 100) -> List[Dict]:
     rows = []
     for p in pairs:
         c = dict(p, nx=nx)
         mesh = case_mesh(c)
         fs = mg.bump_freestream(c["mach"])
-        plain = sur.solve_plain(mesh, fs, tol, precision, max_steps)
-        warm = sur.solve_warm(mesh, fs, mlp, c["mach"], c["h"], tol, precision, max_steps)
+        plain = sur.solve_plain(mesh, fs, tol, precision, max_steps, check_every, limiter=limiter)
+        warm = sur.solve_warm(mesh, fs, mlp, c["mach"], c["h"], tol, precision, max_steps, check_every,
+                              limiter=limiter)
         d = float(np.linalg.norm(warm["U"] - plain["U"]) / np.linalg.norm(plain["U"]))
         d0 = float(np.linalg.norm(warm["U_warm"] - plain["U"]) / np.linalg.norm(plain["U"]))
         rows.append({"mach": c["mach"], "h": c["h"], "cells": mesh.n_cells,
@@ -156,21 +159,21 @@ def evaluate(mlp: sur.MLP, pairs: List[Dict], nx: int, precision: str, tol: floa
     return rows
 
 
-def headline(mlp: sur.MLP, tol: float, max_steps: int) -> Dict:
+def headline(mlp: sur.MLP, tol: float, max_steps: int, limiter: str = "none") -> Dict:
     """Time to a `tol` residual drop on the 3,145,728-tet channel (128 x 64 x 64 hexes, Mach 0.5,
     h = 0.1): FP64 and mixed from the free stream, mixed from the surrogate's warm start, all to
     the same absolute residual."""
     c = {"nx": 128, "mach": 0.5, "h": 0.1}
     mesh = S.Mesh.from_tet_mesh(mg.bump_mesh(128, 64, 64, h=0.1))
     fs = mg.bump_freestream(0.5)
-    out = {"cells": mesh.n_cells}
+    out = {"cells": mesh.n_cells, "limiter": limiter}
     for prec in ("fp64", "mixed"):
-        r = sur.solve_plain(mesh, fs, tol, prec, max_steps, check_every=500)
+        r = sur.solve_plain(mesh, fs, tol, prec, max_steps, check_every=500, limiter=limiter)
         out["plain_" + prec] = {k: v for k, v in r.items() if k != "U"}
         if prec == "mixed":
             U_plain = r["U"]
         print(json.dumps({prec: out["plain_" + prec]}, default=float), flush=True)
-    w = sur.solve_warm(mesh, fs, mlp, c["mach"], c["h"], tol, "mixed", max_steps, check_every=500)
+    w = sur.solve_warm(mesh, fs, mlp, c["mach"], c["h"], tol, "mixed", max_steps, check_every=500, limiter=limiter)
     out["warm_mixed"] = {k: v for k, v in w.items() if k not in ("U", "U_warm")}
     out["warm_final_rel_l2"] = float(np.linalg.norm(w["U"] - U_plain) / np.linalg.norm(U_plain))
     out["warm_start_rel_l2"] = float(np.linalg.norm(w["U_warm"] - U_plain) / np.linalg.norm(U_plain))
@@ -202,6 +205,12 @@ def main(argv=None):
     ap.add_argument("--fine-nx", type=int, default=96)
     ap.add_argument("--eval-pairs", type=int, default=16)
     ap.add_argument("--eval-nx", type=int, default=40)
+    ap.add_argument("--limiter", choices=sorted(sur.STEADY_LIMITERS), default="none",
+                    help="none: the unlimited scheme; barth-ratchet: the reference's Barth limiter, ratcheted "
+                         "once a case's residual has dropped 1e-2 (needed where the flow turns transonic)")
+    ap.add_argument("--eval-check-every", type=int, default=100)
+    ap.add_argument("--load-mlp", default="", help="start from these parameters (.npy) instead of training")
+    ap.add_argument("--skip-sweep", action="store_true", help="with --load-mlp: no sweep, no training")
     ap.add_argument("--out", required=True)
     ap.add_argument("--save-data", default="", help="write the training set (features, targets) to this .npz")
     ap.add_argument("--headline", action="store_true",
@@ -245,11 +254,19 @@ def main(argv=None):
         total_ms = max(t[0] for t in times)
         summary["sweep"] = {"per_case": merged, "cells": int(sum(r["cells"] for r in merged)), "ranks": world,
                             "total_ms": total_ms, "mcell_stages_per_s": work / (total_ms * 1e-3) / 1e6}
+    elif a.skip_sweep:
+        F = T = None
     else:
-        res = run_batched(cases, a.precision, a.tol, a.max_steps)
+        res = run_batched(cases, a.precision, a.tol, a.max_steps, limiter=a.limiter)
         summary["sweep"] = {k: v for k, v in res.items() if k not in ("U", "meshes", "offsets")}
         F, T = training_data(res, cases)
         del res
+    if a.skip_sweep:
+        if not a.load_mlp:
+            raise SystemExit("--skip-sweep needs --load-mlp")
+        mlp = sur.MLP(seed=a.seed)
+        mlp.set_params(np.load(a.load_mlp))
+        return finish(a, summary, mlp, world)
     sw = summary["sweep"]
     print(json.dumps({"sweep_cells": sw["cells"], "total_ms": sw["total_ms"],
                       "mcell_stages_per_s": sw["mcell_stages_per_s"],
@@ -269,10 +286,14 @@ def main(argv=None):
     np.save(os.path.join(a.out, "mlp_params.npy"), mlp.get_params())
     print(json.dumps({"train_ms": tr["ms"], "loss_first": float(tr["loss"][0]), "loss_last": float(tr["loss"][-1])}),
           flush=True)
+    return finish(a, summary, mlp, world)
 
+
+def finish(a, summary: Dict, mlp: sur.MLP, world: int):
+    """Warm-start evaluation on held-out pairs, the optional headline, the summary file."""
     rng = np.random.default_rng(a.seed + 1)
     pairs = [{"mach": float(rng.uniform(*a.mach)), "h": float(rng.uniform(*a.h))} for _ in range(a.eval_pairs)]
-    rows = evaluate(mlp, pairs, a.eval_nx, a.precision, a.tol, a.max_steps)
+    rows = evaluate(mlp, pairs, a.eval_nx, a.precision, a.tol, a.max_steps, a.limiter, a.eval_check_every)
     summary["eval"] = rows
     ok = [r for r in rows if r["time_ratio"] is not None]
     summary["eval_summary"] = {
@@ -281,7 +302,7 @@ def main(argv=None):
         "max_final_rel_l2": float(max(r["final_rel_l2"] for r in rows)) if rows else None,
         "fallbacks": sum(1 for r in rows if r["warm"]["fallback"])}
     if a.headline:
-        summary["headline"] = headline(mlp, a.tol, a.max_steps)
+        summary["headline"] = headline(mlp, a.tol, a.max_steps, a.limiter)
         print(json.dumps(summary["headline"], default=float), flush=True)
     with open(os.path.join(a.out, "summary.json"), "w") as f:
         json.dump(summary, f, indent=1, default=float)
