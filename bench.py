@@ -53,7 +53,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--steady", action="store_true",
-                    help="also time a local-time-stepping solve to a 1e-6 density-residual drop")
+                    help="also time a local-time-stepping solve of the benched channel to a 1e-6 density-residual "
+                         "drop (minutes)")
+    ap.add_argument("--no-steady-quick", action="store_true",
+                    help="skip the quick time-to-solution study on a 24x12x12 channel")
     ap.add_argument("--steady-max", type=int, default=60000)
     ap.add_argument("--steady-limiter", choices=["none", "barth-ratchet"], default="none")
     ap.add_argument("--block", type=int, default=0, help="fix the block size (no tuning)")
@@ -194,11 +197,13 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
 
 
 # DRAM bytes per cell of one launch (dram__bytes_read.sum + dram__bytes_write.sum), captured
-# with ncu on the full 3,145,728-tet bump channel with the tuned launch shapes (FP64: gradient
-# 64/7, flux 64/9; mixed: gradient 64/7, flux 128/8); the bump workload's `roofline.traffic`
-# is this times its cells, other workloads report null.
+# with ncu on the full 3,145,728-tet bump channel with the tuned launch shapes, averaged over the
+# three stages of a step like the event-timed launch durations (FP64: gradient 64/7, flux 64/9,
+# stages 753.9 / 752.4 / 856.0 and 1100.5 / 1212.2 / 1214.9 MB; mixed: gradient 64/7, flux
+# 128/8); the bump workload's `roofline.traffic` is this times its cells, other workloads report
+# null.
 MEASURED_DRAM_BYTES_PER_CELL = {
-    ("fp64", "gradient"): 753.0e6 / 3145728, ("fp64", "flux"): 1099.8e6 / 3145728,
+    ("fp64", "gradient"): 787.4e6 / 3145728, ("fp64", "flux"): 1175.9e6 / 3145728,
     ("mixed", "gradient"): 503.2e6 / 3145728, ("mixed", "flux"): 979.7e6 / 3145728,
 }
 
@@ -337,6 +342,48 @@ def host_link(nbytes: int, reps: int = 5):
     return {"bytes": int(nbytes), "h2d_gbs": round(reps * nbytes / t_in / 1e9, 2),
             "d2h_gbs": round(reps * nbytes / t_out / 1e9, 2),
             "both_total_gbs": round(2 * reps * nbytes / t_both / 1e9, 2)}
+
+
+def steady_quick(device: int):
+    """Time to a 1e-6 density-residual drop on a small channel (24 x 12 x 12 hexes, 20,736 tets,
+    Mach 0.5, h = 0.1, unlimited scheme, local time stepping at CFL 0.8), measured in this run:
+    FP64 and mixed from the free stream, and mixed from the surrogate's warm start, the network
+    trained in this run (3,000 Adam steps) on 8 converged channels of 16..22 hexes in x that do not
+    include the evaluated one. All three solves stop at the same absolute residual (1e-6 of the
+    free-stream start's first residual); times are device times of the solves (the warm start's
+    includes its preparation)."""
+    from netflux_b200 import meshgen as mg
+    from netflux_b200 import surrogate as sur
+    from netflux_b200 import sweep as SW
+    t0 = time.perf_counter()
+    cases = SW.sample_cases(8, 3, 16, 22, (0.35, 0.65), (0.05, 0.12))
+    res = SW.run_batched(cases, "mixed", 1e-6, 100000, 50, device=device)
+    F, T = SW.training_data(res, cases)
+    mlp = sur.MLP(seed=1)
+    mlp.set_data(F, T)
+    tr = mlp.train_schedule(3000, 16384, 1e-3, seed=1, n_report=3)
+    c = {"nx": 24, "mach": 0.5, "h": 0.1}
+    mesh = SW.case_mesh(c)
+    fs = mg.bump_freestream(c["mach"])
+    out = {"workload": "bump channel 24x12x12 hexes, 6 tets each (20,736 tets), Mach 0.5, h 0.1, limiter none",
+           "tol": 1e-6, "training": {"cases": len(cases), "samples": int(F.shape[0]), "steps": 3000,
+                                     "loss": float(tr["loss"][-1]), "ms": round(float(tr["ms"]), 1)}}
+    plain = {}
+    for prec in ("fp64", "mixed"):
+        r = sur.solve_plain(mesh, fs, 1e-6, prec, 200000, 50)
+        plain[prec] = r
+        out["plain_" + prec] = {"steps": r["steps"], "ms": round(r["ms"], 2), "converged": r["converged"]}
+    w = sur.solve_warm(mesh, fs, mlp, c["mach"], c["h"], 1e-6, "mixed", 200000, 50)
+    ms_w = w["ms"] + 1e3 * w["prep_s"]
+    out["warm_mixed"] = {"steps": w["steps"], "ms": round(ms_w, 2), "converged": w["converged"],
+                         "fallback": w["fallback"]}
+    out["time_ratio_mixed_vs_fp64"] = round(plain["mixed"]["ms"] / plain["fp64"]["ms"], 4)
+    out["time_ratio_warm_mixed_vs_fp64"] = round(ms_w / plain["fp64"]["ms"], 4)
+    out["warm_final_rel_l2_vs_plain_mixed"] = float(np.linalg.norm(w["U"] - plain["mixed"]["U"]) /
+                                                    np.linalg.norm(plain["mixed"]["U"]))
+    out["wall_s"] = round(time.perf_counter() - t0, 1)
+    mlp.close()
+    return out
 
 
 def main():
@@ -501,6 +548,10 @@ def main():
                   "res_final": float(out["res"][0]),
                   "drop": float(out["res"][0] / out["res0"][0]) if out["res0"][0] > 0 else None}
 
+    quick = None
+    if rank == 0 and world == 1 and not args.no_steady_quick:
+        quick = steady_quick(local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # the same workload and mesh
@@ -531,6 +582,8 @@ def main():
             "gpu_launches": int(round(kernels_per_step * args.steps)),
             "cpu_baseline": cpu,
         }
+        if quick is not None:
+            line["steady_quick"] = quick
         if steady is not None:
             line["steady"] = steady
         print(json.dumps(line))

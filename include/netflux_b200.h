@@ -113,6 +113,17 @@ nf_mesh* nf_mesh_from_su2(const char* path, int n_patch_types, const char* const
 nf_mesh* nf_mesh_from_arrays(int64_t n_nodes, const double* nodes, int64_t n_cells, const int64_t* tets,
                              int n_markers, const char* const* marker_names, const int* marker_types,
                              const int64_t* marker_offsets, const int64_t* marker_tris);
+/* The same grid built on a CUDA device (device < 0: the current one): face
+ * matching by sorting on the GPU instead of FV_Grid's std::map
+ * (FV_Grid.cpp:38-64), the reference's face order (Faces::sort,
+ * GeometryUtilities.cpp:484-513), the geometry of FV_Grid.cpp:154-205 and
+ * GeometryUtilities.cpp:289-325, calc_Delta_S (Solver.cpp:276-298) and the
+ * Hilbert renumbering, all as kernels with the host builder's rounding. The
+ * resulting mesh equals nf_mesh_from_arrays's bit for bit, and invalid input
+ * gives the same error text. */
+nf_mesh* nf_mesh_from_arrays_device(int64_t n_nodes, const double* nodes, int64_t n_cells, const int64_t* tets,
+                                    int n_markers, const char* const* marker_names, const int* marker_types,
+                                    const int64_t* marker_offsets, const int64_t* marker_tris, int device);
 
 /* Concatenate meshes into one batched mesh (cells, faces and patches of case
  * b follow those of case b-1). Every case keeps its own patches. */
@@ -236,6 +247,24 @@ int nf_set_state_old(nf_solver* s, const double* U_old, int64_t n_cells);
 int nf_calc_timestep(nf_solver* s, double* dt_out);
 int nf_set_timestep(nf_solver* s, double dt);
 int nf_step(nf_solver* s);
+/* One stage of a step (0, 1, 2 for TVD-RK3; 0 for explicit Euler), in order;
+ * the last stage ends the step as nf_step does. Between stages the caller may
+ * exchange halo primitives (nf_halo_pack / nf_halo_unpack) with the solvers
+ * of the other parts of a mesh split across solvers. NF_ERR_ARG out of
+ * order; nf_step and nf_advance refuse while a step begun here is open.
+ * Stage-wise time integration has no counterpart in the reference, which
+ * runs TVD_RK3 as one call (Solver.cpp:103-133). */
+int nf_stage(nf_solver* s, int stage);
+/* Halo exchange of a mesh split across solvers (one per part, each part with
+ * two layers of halo cells; netflux_b200/partition.py builds the parts and
+ * the exchange plan): nf_halo_pack gathers the primitives the next stage
+ * reads, of the n cells listed (device numbering, int64 on the device), into
+ * the device buffer buf [5][n]; nf_halo_unpack writes such a buffer into the
+ * listed cells. Both run on the solver's stream and return when done. No
+ * counterpart in the reference (its MPI decomposition is a commented-out
+ * sketch, Decomposition.cpp:3-51). */
+int nf_halo_pack(nf_solver* s, const int64_t* cells, int64_t n, double* buf);
+int nf_halo_unpack(nf_solver* s, const int64_t* cells, int64_t n, const double* buf);
 /* n_steps x (calc_timestep + step) on the device; time (may be NULL) returns
  * the accumulated time. Uses a CUDA graph after the first call. */
 int nf_advance(nf_solver* s, int64_t n_steps, double* time_out);

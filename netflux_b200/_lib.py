@@ -12,7 +12,11 @@ from typing import Optional
 
 import numpy as np
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libnetflux_b200.so")
+# NETFLUX_B200_DEBUG=1 loads the NF_DEBUG build (make -C netflux_b200/csrc debug), whose kernels check
+# every mesh index they read and report one out of range as NF_ERR_MESH.
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib",
+                        "libnetflux_b200_debug.so" if os.environ.get("NETFLUX_B200_DEBUG") == "1"
+                        else "libnetflux_b200.so")
 
 NF_OK, NF_ERR_ARG, NF_ERR_MESH, NF_ERR_CUDA, NF_ERR_NONPHYSICAL, NF_ERR_DT, NF_ERR_UNSUPPORTED = range(7)
 NF_BC_NO_SLIP_WALL, NF_BC_SLIP_WALL, NF_BC_FAR_FIELD = 0, 1, 2
@@ -26,10 +30,10 @@ NF_PREC_FP64_REF, NF_PREC_FP64, NF_PREC_MIXED = 0, 1, 2
 
 # Every symbol the header declares (checked by the CPU test suite).
 EXPORTED = (
-    "nf_mesh_from_su2", "nf_mesh_from_arrays", "nf_mesh_concat", "nf_mesh_get_info", "nf_mesh_get_patch",
+    "nf_mesh_from_su2", "nf_mesh_from_arrays", "nf_mesh_from_arrays_device", "nf_mesh_concat", "nf_mesh_get_info", "nf_mesh_get_patch",
     "nf_mesh_export", "nf_mesh_get_permutation", "nf_mesh_get_case_offsets", "nf_mesh_destroy",
     "nf_params_default", "nf_create", "nf_set_state", "nf_get_state", "nf_set_state_old", "nf_calc_timestep", "nf_set_timestep",
-    "nf_step", "nf_advance", "nf_get_residual", "nf_get_field", "nf_synchronize", "nf_last_error", "nf_destroy",
+    "nf_step", "nf_stage", "nf_halo_pack", "nf_halo_unpack", "nf_advance", "nf_get_residual", "nf_get_field", "nf_synchronize", "nf_last_error", "nf_destroy",
     "nf_time_steps", "nf_residual_norms_noalloc", "nf_tune", "nf_set_launch_shapes", "nf_snapshot_begin", "nf_snapshot_wait", "nf_upload_begin", "nf_upload_commit", "nf_upload_wait", "nf_solve_steady", "nf_solve_steady_to", "nf_fastmath_selftest", "nf_check_mesh_size", "nf_set_host_threads",
     "nf_mlp_param_count", "nf_mlp_create", "nf_mlp_last_error", "nf_mlp_destroy", "nf_mlp_get_params",
     "nf_mlp_set_params", "nf_mlp_set_data", "nf_mlp_train", "nf_mlp_gradients", "nf_mlp_predict",
@@ -83,6 +87,7 @@ def load() -> C.CDLL:
     sig = {
         "nf_mesh_from_su2": (P, [C.c_char_p, I, C.POINTER(C.c_char_p), C.POINTER(C.c_int)]),
         "nf_mesh_from_arrays": (P, [I64, dp, I64, i64p, I, C.POINTER(C.c_char_p), C.POINTER(C.c_int), i64p, i64p]),
+        "nf_mesh_from_arrays_device": (P, [I64, dp, I64, i64p, I, C.POINTER(C.c_char_p), C.POINTER(C.c_int), i64p, i64p, I]),
         "nf_mesh_concat": (P, [I, C.POINTER(P)]),
         "nf_mesh_get_info": (I, [P, C.POINTER(NfMeshInfo)]),
         "nf_mesh_get_patch": (I, [P, I, C.POINTER(C.c_int), i64p, i64p, C.POINTER(C.c_int), C.c_char_p, C.c_size_t]),
@@ -98,6 +103,9 @@ def load() -> C.CDLL:
         "nf_calc_timestep": (I, [P, dp]),
         "nf_set_timestep": (I, [P, D]),
         "nf_step": (I, [P]),
+        "nf_stage": (I, [P, I]),
+        "nf_halo_pack": (I, [P, P, I64, P]),
+        "nf_halo_unpack": (I, [P, P, I64, P]),
         "nf_advance": (I, [P, I64, dp]),
         "nf_get_residual": (I, [P, dp, I]),
         "nf_get_field": (I, [P, I, dp, I64]),

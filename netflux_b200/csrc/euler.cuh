@@ -25,6 +25,7 @@ enum : unsigned {
   kErrNonFinite = 1u,     // a non-finite residual or state
   kErrNonPhysical = 2u,   // rho <= 0 or p <= 0 after an update
   kErrDt = 4u,            // a cell produced dt <= 0
+  kErrIndex = 8u,         // NF_DEBUG builds: a mesh index out of range (the access was redirected)
 };
 
 template <typename T>

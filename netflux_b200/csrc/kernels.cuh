@@ -64,7 +64,35 @@ struct MeshView {
   const int* __restrict__ b_face;  // face id (geometry)
   const int* __restrict__ b_patch; // patch
   const int* __restrict__ b_fs;    // face-state slot of the owner (slot order of the kernels in use)
+  int n_nodes;                     // for the index checks of NF_DEBUG builds
+  int n_patches;
 };
+
+// Index checks of NF_DEBUG builds (make debug): every index a kernel reads
+// from the mesh arrays is checked before it is used; an index out of range
+// sets kErrIndex in the status word and is replaced by a valid one (0, or the
+// cell itself), so the access stays in bounds and the host reports the error.
+// In the release build these are the identity.
+__device__ __forceinline__ int checked(int idx, int limit, unsigned* status) {
+#ifdef NF_DEBUG
+  if (idx < 0 || idx >= limit) {
+    atomicOr(status, kErrIndex);
+    return 0;
+  }
+#endif
+  return idx;
+}
+// a neighbour code: cell << shift (| slot) below n cells, or -(1 + boundary face) below nb
+__device__ __forceinline__ int checked_nb(int code, int shift, int n, int nb, int self, unsigned* status) {
+#ifdef NF_DEBUG
+  const bool ok = code >= 0 ? (code >> shift) < n : (-code - 1) < nb;
+  if (!ok) {
+    atomicOr(status, kErrIndex);
+    return self;
+  }
+#endif
+  return code;
+}
 
 struct StageArgs {
   int second_order;      // SpatialOrder::Second
@@ -223,7 +251,8 @@ __global__ void __launch_bounds__(256) gradient_limiter_kernel(MeshView<T> m, St
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     sl[q] = m.slot[q * st + c];
-    ns[q] = m.nbslot[q * st + c];
+    sl[q] = sl[q] < 0 ? -1 : (checked(sl[q] >> 1, F, a.status) << 1 | (sl[q] & 1));
+    ns[q] = checked_nb(m.nbslot[q * st + c], 2, m.n, m.nb, c << 2, a.status);
   }
   const T vc = ld_v<T>(a, k * st + c);
   const T vol = T(m.vol[c]);
@@ -319,8 +348,9 @@ __global__ void __launch_bounds__(256) flux_update_kernel(MeshView<T> m, StageAr
   const int st = m.stride;
   const int F = m.n_faces;
   const bool second = a.second_order != 0;
-  const int sl = m.slot[q * st + c];
-  const int ns = m.nbslot[q * st + c];
+  int sl = m.slot[q * st + c];
+  sl = sl < 0 ? -1 : (checked(sl >> 1, F, a.status) << 1 | (sl & 1));
+  const int ns = checked_nb(m.nbslot[q * st + c], 2, m.n, m.nb, c << 2 | q, a.status);
   const bool has = sl >= 0;
   const bool own = (sl & 1) == 0;
   // this face's contribution to R: -F on the owner side, +F on the other
@@ -443,7 +473,11 @@ __device__ __forceinline__ void block_min_to(double v, unsigned long long* targe
     v = (lane < int(blockDim.x + 31) / 32) ? wmin[lane] : DBL_MAX;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, off));
-    if (lane == 0 && v < DBL_MAX) atomicMin(target, (unsigned long long)__double_as_longlong(v));
+    // a block whose minimum is not below the current one skips the atomic
+    // (the value only decreases, so the result is the same exact minimum)
+    if (lane == 0 && v < DBL_MAX &&
+        v < __longlong_as_double(static_cast<long long>(*reinterpret_cast<volatile unsigned long long*>(target))))
+      atomicMin(target, (unsigned long long)__double_as_longlong(v));
   }
 }
 
@@ -495,10 +529,10 @@ __device__ __forceinline__ void prefetch_update_rows(const StageArgs& a, int c, 
 // a record starts on 32 bytes (FP64) or 16 bytes (FP32): x and y come in one
 // 16-byte load (FP64), or the whole record in one (FP32).
 template <typename T>
-__device__ __forceinline__ void load_vertices(const MeshView<T>& m, int c, T P[4][3]) {
+__device__ __forceinline__ void load_vertices(const MeshView<T>& m, int c, T P[4][3], unsigned* status) {
 #pragma unroll
   for (int v = 0; v < 4; v++) {
-    const int id = m.cnode[v * m.stride + c];
+    const int id = checked(m.cnode[v * m.stride + c], m.n_nodes, status);
     const T* p = m.nodes + 4 * size_t(id);
     if constexpr (sizeof(T) == 8) {
       const double2 xy = *reinterpret_cast<const double2*>(p);
@@ -550,7 +584,7 @@ __device__ __forceinline__ void gradient_node_cell(const MeshView<T>& m, const S
   T* __restrict__ fsc = a.fs + c;  // this cell's column of the face states
   int nb[4];
 #pragma unroll
-  for (int q = 0; q < 4; q++) nb[q] = m.nbvf[q * st + c];
+  for (int q = 0; q < 4; q++) nb[q] = checked_nb(m.nbvf[q * st + c], 0, m.n, m.nb, c, a.status);
   auto fetch = [&](int k, T& vc, T vo[4]) {
     const T* Vk = Vin + k * st;
     vc = Vk[c];
@@ -583,7 +617,7 @@ __device__ __forceinline__ void gradient_node_cell(const MeshView<T>& m, const S
   T S[4][3], d[4][3];  // outward normals; (centroid - P_m) / 3
   {
     T P[4][3];
-    load_vertices(m, c, P);
+    load_vertices(m, c, P, a.status);
     face_normals(P, S);
     const T cen[3] = {T(0.25) * ((P[0][0] + P[1][0]) + (P[2][0] + P[3][0])),
                       T(0.25) * ((P[0][1] + P[1][1]) + (P[2][1] + P[3][1])),
@@ -683,6 +717,10 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
   pdl_wait_previous();
   const bool in = c < m.n;
   const bool active = in && !frozen_cell(a, c);
+  if (kDt && active) {  // the time step's own rows: into L2 now, read after the gradient work
+#pragma unroll
+    for (int e = 0; e < 3; e++) prefetch_l2(m.dS + size_t(e) * m.stride + c);
+  }
   T vown[5];
   if (active) gradient_node_cell<T, kPipe>(m, a, c, vown);
   if constexpr (kDt) {
@@ -771,7 +809,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
   const int code = m.gcode[c];
   int ns[4];
 #pragma unroll
-  for (int q = 0; q < 4; q++) ns[q] = m.nbsf[q * st + c];
+  for (int q = 0; q < 4; q++) ns[q] = checked_nb(m.nbsf[q * st + c], 2, m.n, m.nb, c << 2 | q, a.status);
   auto fetch = [&](int q, FaceIn<T>& in) {
     const int bits = code >> (3 * q);
     if ((bits & 1) == 0) {
@@ -809,7 +847,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
   T S[4][3];
   {
     T P[4][3];
-    load_vertices(m, c, P);
+    load_vertices(m, c, P, a.status);
     face_normals(P, S);
   }
   double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -862,13 +900,13 @@ __global__ void __launch_bounds__(256) ghost_kernel(MeshView<T> m, StageArgs a) 
   pdl_launch_dependents();
   pdl_wait_previous();
   if (b >= m.nb) return;
-  const int c = m.b_cell[b], f = m.b_face[b];
+  const int c = checked(m.b_cell[b], m.n, a.status), f = checked(m.b_face[b], m.n_faces, a.status);
   const int F = m.n_faces, st = m.stride;
   T V[5], G[5];
 #pragma unroll
   for (int k = 0; k < 5; k++) V[k] = ld_v<T>(a, k * st + c);
   const T nh[3] = {m.nhat[f], m.nhat[F + f], m.nhat[2 * F + f]};
-  ghost_state<T>(m.patches[m.b_patch[b]], V, nh, G);
+  ghost_state<T>(m.patches[checked(m.b_patch[b], m.n_patches, a.status)], V, nh, G);
 #pragma unroll
   for (int k = 0; k < 5; k++) {
     a.vg[k * m.bstride + b] = G[k];
@@ -881,7 +919,8 @@ __global__ void __launch_bounds__(256) boundary_flux_kernel(MeshView<T> m, Stage
   pdl_launch_dependents();
   pdl_wait_previous();
   if (b >= m.nb) return;
-  const int c = m.b_cell[b], q = m.b_fs[b], f = m.b_face[b];
+  const int c = checked(m.b_cell[b], m.n, a.status), q = checked(m.b_fs[b], 4, a.status),
+            f = checked(m.b_face[b], m.n_faces, a.status);
   const int F = m.n_faces, st = m.stride;
   T VL[5], VR[5];
 #pragma unroll
@@ -893,7 +932,7 @@ __global__ void __launch_bounds__(256) boundary_flux_kernel(MeshView<T> m, Stage
     }
   }
   const T nh[3] = {m.nhat[f], m.nhat[F + f], m.nhat[2 * F + f]};
-  ghost_state<T>(m.patches[m.b_patch[b]], VL, nh, VR);
+  ghost_state<T>(m.patches[checked(m.b_patch[b], m.n_patches, a.status)], VL, nh, VR);
   T Fl[5];
   if constexpr (kRef) {
     T UL[5], UR[5];

@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshVie
   float* __restrict__ inc_c = a.fs32 + c;  // this cell's column of the increments
   int nb[4];
 #pragma unroll
-  for (int q = 0; q < 4; q++) nb[q] = m.nbvf[q * st + c];
+  for (int q = 0; q < 4; q++) nb[q] = checked_nb(m.nbvf[q * st + c], 0, m.n, m.nb, c, a.status);
   auto fetch = [&](int k, double& vc, double vo[4]) {
     const double* Vk = V + size_t(k) * st;
     vc = Vk[c];
@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_delta_kernel(MeshVie
   float S[4][3], d[4][3];  // outward normals; (centroid - P_m) / 3
   {
     float P[4][3];
-    load_vertices(m, c, P);
+    load_vertices(m, c, P, a.status);
     face_normals(P, S);
     const float cen[3] = {0.25f * ((P[0][0] + P[1][0]) + (P[2][0] + P[3][0])),
                           0.25f * ((P[0][1] + P[1][1]) + (P[2][1] + P[3][1])),
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_delta_kernel(MeshView<fl
   }
   int ns[4];
 #pragma unroll
-  for (int q = 0; q < 4; q++) ns[q] = m.nbsf[q * st + c];
+  for (int q = 0; q < 4; q++) ns[q] = checked_nb(m.nbsf[q * st + c], 2, m.n, m.nb, c << 2 | q, a.status);
   // kind 0 no face, 1 interior, 3 boundary; s: own increments or the
   // boundary flux difference; x: the other side's state minus V_c
   auto fetch = [&](int q, FaceIn<float>& in) {
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_delta_kernel(MeshView<fl
   float S[4][3];
   {
     float P[4][3];
-    load_vertices(m, c, P);
+    load_vertices(m, c, P, a.status);
     face_normals(P, S);
   }
   double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -331,7 +331,8 @@ __global__ void __launch_bounds__(256) boundary_flux_delta_kernel(MeshView<doubl
   pdl_launch_dependents();
   pdl_wait_previous();
   if (b >= m.nb) return;
-  const int c = m.b_cell[b], q = m.b_fs[b], f = m.b_face[b];
+  const int c = checked(m.b_cell[b], m.n, a.status), q = checked(m.b_fs[b], 4, a.status),
+            f = checked(m.b_face[b], m.n_faces, a.status);
   const int F = m.n_faces, st = m.stride;
   double Vc[5], VL[5], VR[5];
 #pragma unroll
@@ -341,7 +342,7 @@ __global__ void __launch_bounds__(256) boundary_flux_delta_kernel(MeshView<doubl
   }
   const double nh[3] = {m.nhat[f], m.nhat[F + f], m.nhat[2 * F + f]};
   const double area = m.area[f];
-  ghost_state<double>(m.patches[m.b_patch[b]], VL, nh, VR);
+  ghost_state<double>(m.patches[checked(m.b_patch[b], m.n_patches, a.status)], VL, nh, VR);
   double Fl[5];
   rusanov_fast<double>(VL, VR, nh, area, Fl);
   // area F(V_c) . n

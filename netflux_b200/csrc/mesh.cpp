@@ -9,6 +9,7 @@
 // Compiled with -ffp-contract=off: the geometry must round exactly as the
 // reference's (no fused multiply-add on the x86-64 baseline it targets).
 #include "mesh.hpp"
+#include "mesh_common.hpp"
 
 #include "../../include/netflux_b200.h"
 
@@ -105,51 +106,13 @@ inline V3 node(const std::vector<double>& nodes, int64_t n) {
   return {nodes[3 * n], nodes[3 * n + 1], nodes[3 * n + 2]};
 }
 
-// Local faces of a tetrahedron, get_face_element_k_of_tetrahedron
-// (GeometryUtilities.cpp:71-101).
-constexpr int kTetFace[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
-
 struct FaceKey {
   uint64_t hi, lo;  // sorted node ids (a<<32|b, c<<32|payload)
 };
 
-inline void sort3(uint32_t& a, uint32_t& b, uint32_t& c) {
-  if (a > b) std::swap(a, b);
-  if (b > c) std::swap(b, c);
-  if (a > b) std::swap(a, b);
-}
-
-// ---- 3-D Hilbert index (Skilling, "Programming the Hilbert curve", AIP
-// Conf. Proc. 707, 2004: axes -> transposed index, then bit interleave) ----
-uint64_t hilbert3(uint32_t x, uint32_t y, uint32_t z, int bits) {
-  uint32_t X[3] = {x, y, z};
-  const uint32_t M = 1u << (bits - 1);
-  for (uint32_t Q = M; Q > 1; Q >>= 1) {  // inverse undo
-    const uint32_t P = Q - 1;
-    for (int i = 0; i < 3; i++) {
-      if (X[i] & Q) {
-        X[0] ^= P;
-      } else {
-        uint32_t t = (X[0] ^ X[i]) & P;
-        X[0] ^= t;
-        X[i] ^= t;
-      }
-    }
-  }
-  for (int i = 1; i < 3; i++) X[i] ^= X[i - 1];  // Gray encode
-  uint32_t t = 0;
-  for (uint32_t Q = M; Q > 1; Q >>= 1)
-    if (X[2] & Q) t ^= Q - 1;
-  for (int i = 0; i < 3; i++) X[i] ^= t;
-  uint64_t h = 0;
-  for (int b = bits - 1; b >= 0; b--)
-    for (int i = 0; i < 3; i++) h = (h << 1) | ((X[i] >> b) & 1u);
-  return h;
-}
-
 // Hilbert order of the cells [begin, end) (reference numbering) by centroid.
 void hilbert_renumber(Mesh& m, int64_t begin, int64_t end) {
-  const int bits = 21;
+  const int bits = kHilbertBits;
   double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   for (int64_t c = begin; c < end; c++)
     for (int d = 0; d < 3; d++) {

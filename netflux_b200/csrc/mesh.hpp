@@ -69,4 +69,15 @@ Mesh read_su2(const std::string& path, const std::vector<std::string>& names, co
 
 Mesh concat_meshes(const std::vector<const Mesh*>& parts);
 
+// The same Mesh, bit for bit, built on the current CUDA device
+// (mesh_device.cu): face matching, orderings, geometry and the Hilbert
+// renumbering run as kernels; the result is copied back to the host.
+Mesh build_mesh_device(const std::vector<double>& nodes, const std::vector<int64_t>& tets,
+                       const std::vector<MarkerInput>& markers);
+
 }  // namespace nf
+
+// The C ABI's opaque mesh handle (include/netflux_b200.h).
+struct nf_mesh {
+  nf::Mesh m;
+};

@@ -25,9 +25,6 @@
 #include "launch.hpp"
 #include "mesh.hpp"
 
-struct nf_mesh {
-  nf::Mesh m;
-};
 
 namespace {
 
@@ -142,6 +139,25 @@ __global__ void residual_finalize_kernel(const double* __restrict__ part, const 
   out[2 * cs + 1] = mx;
 }
 
+// Halo exchange of a mesh split across solvers: the stage-input primitives of
+// listed cells (device order) gathered into / scattered from [5][n] rows.
+__global__ void halo_pack_kernel(int64_t n, int st, const int64_t* __restrict__ cells, const double* __restrict__ V,
+                                 double* __restrict__ buf) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t c = cells[i];
+#pragma unroll
+  for (int k = 0; k < 5; k++) buf[k * n + i] = V[size_t(k) * st + c];
+}
+__global__ void halo_unpack_kernel(int64_t n, int st, const int64_t* __restrict__ cells,
+                                   const double* __restrict__ buf, double* __restrict__ V) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t c = cells[i];
+#pragma unroll
+  for (int k = 0; k < 5; k++) V[size_t(k) * st + c] = buf[k * n + i];
+}
+
 // AoS state in reference cell order <-> SoA in device order.
 __global__ void scatter_state_kernel(int n, int st, const long long* __restrict__ dev_of_ref,
                                      const double* __restrict__ aos, double* __restrict__ soa) {
@@ -198,6 +214,7 @@ struct nf_solver {
   cudaStream_t stream = nullptr;
   nf_params p{};
   int n = 0, stride = 0, n_faces = 0, n_cases = 1;
+  int64_t n_nodes = 0;
   int block = 256;
   std::vector<int64_t> dev_of_ref;
   std::vector<int64_t> case_offsets;
@@ -318,12 +335,14 @@ struct nf_solver {
     const bool fast = p.precision != NF_PREC_FP64_REF;
     return nf::MeshView<double>{n, stride, n_faces, slot.p, nbslot.p, S.p, nhat.p, area.p, rs.p,
                                 nodes4.p, cnode.p, gcode.p, nbvf.p, nbsf.p, vol.p, dS.p, patches.p, nb,
-                                bstride, b_cell.p, b_slot.p, b_face.p, b_patch.p, fast ? b_slotf.p : b_slot.p};
+                                bstride, b_cell.p, b_slot.p, b_face.p, b_patch.p, fast ? b_slotf.p : b_slot.p,
+                                int(n_nodes), int(patches.n)};
   }
   nf::MeshView<float> view32() const {
     return nf::MeshView<float>{n, stride, n_faces, slot.p, nbslot.p, nullptr, nullptr, nullptr, nullptr,
                                nodes4_32.p, cnode.p, gcode.p, nbvf.p, nbsf.p, vol.p, dS.p, patches.p, nb,
-                               bstride, b_cell.p, b_slot.p, b_face.p, b_patch.p, b_slotf.p};
+                               bstride, b_cell.p, b_slot.p, b_face.p, b_patch.p, b_slotf.p, int(n_nodes),
+                               int(patches.n)};
   }
 
   void enqueue_dt() {
@@ -527,12 +546,21 @@ struct nf_solver {
       }
   }
 
+  int n_stages() const { return p.time_scheme == NF_TVD_RK3 ? 3 : 1; }
+  int stage_next = 0;  // the next stage nf_stage may enqueue
+
   void enqueue_step() {
-    const int n_stages = p.time_scheme == NF_TVD_RK3 ? 3 : 1;
+    for (int s = 0; s < n_stages(); s++) enqueue_stage(s);
+    stage_next = 0;
+  }
+
+  // One stage of the step; the last one also ends the step.
+  void enqueue_stage(int s) {
+    const int n_stages = this->n_stages();
     const bool fuse = fuse_dt();
     nf::DtFuse dtf{p.cfl, p.local_time_stepping ? dtl(1 - dtl_cur) : nullptr,
                    reinterpret_cast<unsigned long long*>(scal.p + nf::kScalDtNext)};
-    for (int s = 0; s < n_stages; s++) {
+    {
       nf::StageArgs a{};
       a.second_order = p.spatial_order == NF_SECOND_ORDER;
       a.barth = p.limiter == NF_LIMITER_BARTH;
@@ -599,6 +627,7 @@ struct nf_solver {
       prof_end();
       vcur = 1 - vcur;
     }
+    if (s < n_stages - 1) return;
     prof_begin(NF_KERNEL_OTHER);
     scal_kernel<<<1, 1, 0, stream>>>(scal.p, fuse ? 2 : 1, status.p);
     prof_end();
@@ -627,6 +656,10 @@ struct nf_solver {
       err = "Invalid dt calculated";
       return NF_ERR_DT;
     }
+    if (st & nf::kErrIndex) {
+      err = "a mesh index read by a kernel is out of range (checked in the NF_DEBUG build)";
+      return NF_ERR_MESH;
+    }
     return NF_OK;
   }
 
@@ -641,6 +674,7 @@ struct nf_solver {
     vcur = 0;
     dtl_cur = 0;
     dt_ready = false;
+    stage_next = 0;
     stepped = false;
     old_pending = false;
     steps_done = 0;
@@ -875,6 +909,7 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     s->n = int(N);
     s->stride = int((N + 63) / 64 * 64);
     s->n_faces = int(F);
+    s->n_nodes = m.n_nodes;
     s->dev_of_ref = m.dev_of_ref;
     s->case_offsets = m.case_offsets;
     s->n_cases = m.n_cases();
@@ -1368,6 +1403,10 @@ int nf_set_timestep(nf_solver* s, double dt) {
 
 int nf_step(nf_solver* s) {
   return guarded(s, [&]() -> int {
+    if (s->stage_next != 0) {
+      s->err = "nf_step: a step begun with nf_stage is not finished";
+      return NF_ERR_ARG;
+    }
     s->ratchet_due(1);
     s->enqueue_step();
     s->steps_done++;
@@ -1376,9 +1415,59 @@ int nf_step(nf_solver* s) {
   });
 }
 
+int nf_stage(nf_solver* s, int stage) {
+  return guarded(s, [&]() -> int {
+    if (stage != s->stage_next) {
+      s->err = "nf_stage: stage " + std::to_string(stage) + " out of order (next is " +
+               std::to_string(s->stage_next) + ")";
+      return NF_ERR_ARG;
+    }
+    if (stage == 0) s->ratchet_due(1);
+    s->enqueue_stage(stage);
+    s->stage_next = (stage + 1) % s->n_stages();
+    if (s->stage_next == 0) s->steps_done++;
+    ck(cudaGetLastError(), "stage launch");
+    return NF_OK;
+  });
+}
+
+static int halo_args(nf_solver* s, const int64_t* cells, int64_t n, const double* buf, const char* what) {
+  if (n < 0 || (n > 0 && (!cells || !buf))) {
+    s->err = std::string(what) + ": null pointer or negative count";
+    return NF_ERR_ARG;
+  }
+  return NF_OK;
+}
+
+int nf_halo_pack(nf_solver* s, const int64_t* cells, int64_t n, double* buf) {
+  return guarded(s, [&]() -> int {
+    int rc = halo_args(s, cells, n, buf, "nf_halo_pack");
+    if (rc != NF_OK || n == 0) return rc;
+    halo_pack_kernel<<<int((n + 255) / 256), 256, 0, s->stream>>>(n, s->stride, cells, s->Vbuf(s->vcur), buf);
+    ck(cudaGetLastError(), "halo pack");
+    ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
+    return NF_OK;
+  });
+}
+
+int nf_halo_unpack(nf_solver* s, const int64_t* cells, int64_t n, const double* buf) {
+  return guarded(s, [&]() -> int {
+    int rc = halo_args(s, cells, n, buf, "nf_halo_unpack");
+    if (rc != NF_OK || n == 0) return rc;
+    halo_unpack_kernel<<<int((n + 255) / 256), 256, 0, s->stream>>>(n, s->stride, cells, buf, s->Vbuf(s->vcur));
+    ck(cudaGetLastError(), "halo unpack");
+    ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
+    return NF_OK;
+  });
+}
+
 int nf_advance(nf_solver* s, int64_t n_steps, double* time_out) {
   return guarded(s, [&]() -> int {
     if (n_steps < 0) return NF_ERR_ARG;
+    if (s->stage_next != 0) {
+      s->err = "nf_advance: a step begun with nf_stage is not finished";
+      return NF_ERR_ARG;
+    }
     s->run_steps(n_steps);
     ck(cudaGetLastError(), "advance launch");
     int rc = s->check_status();

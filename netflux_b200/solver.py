@@ -145,7 +145,9 @@ class Mesh:
         return cls(L.load().nf_mesh_from_su2(path.encode(), len(names), arr_n, arr_t))
 
     @classmethod
-    def from_tet_mesh(cls, m: TetMesh) -> "Mesh":
+    def from_tet_mesh(cls, m: TetMesh, device: Optional[int] = None) -> "Mesh":
+        """Build the grid from a TetMesh on the host, or with ``device`` (a CUDA device ordinal, -1 the
+        current one) on the GPU; both give the same grid bit for bit."""
         nodes = np.ascontiguousarray(m.nodes, dtype=np.float64)
         tets = np.ascontiguousarray(m.tets, dtype=np.int64)
         names = [n for n, _ in m.markers]
@@ -157,9 +159,11 @@ class Mesh:
                                     else np.zeros((0, 3)), dtype=np.int64)
         arr_n = (C.c_char_p * len(names))(*[n.encode() for n in names])
         arr_t = (C.c_int * len(names))(*types)
-        h = L.load().nf_mesh_from_arrays(nodes.shape[0], L.dptr(nodes), tets.shape[0], L.i64ptr(tets), len(names),
-                                         arr_n, arr_t, L.i64ptr(offs), L.i64ptr(tris))
-        return cls(h)
+        args = (nodes.shape[0], L.dptr(nodes), tets.shape[0], L.i64ptr(tets), len(names), arr_n, arr_t,
+                L.i64ptr(offs), L.i64ptr(tris))
+        if device is None:
+            return cls(L.load().nf_mesh_from_arrays(*args))
+        return cls(L.load().nf_mesh_from_arrays_device(*args, int(device)))
 
     @classmethod
     def concat(cls, meshes: Sequence["Mesh"]) -> "Mesh":

@@ -273,3 +273,34 @@ def training_set(cases, precision: str = "mixed", tol: float = 1e-6, max_steps: 
         T.append(normalise_state(r["U"], fs))
         recs.append({k: v for k, v in r.items() if k != "U"})
     return np.concatenate(F), np.concatenate(T), recs
+
+
+def main(argv=None) -> None:
+    """Time the network's training step (python -m netflux_b200.surrogate --train-bench): Adam steps
+    of `--batch` samples drawn from `--samples` random inputs and targets, a CUDA graph per step."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train-bench", action="store_true", required=True)
+    ap.add_argument("--samples", type=int, default=400000)
+    ap.add_argument("--batch", type=int, default=65536)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    a = ap.parse_args(argv)
+    rng = np.random.default_rng(0)
+    f = rng.uniform(-1, 1, (a.samples, 7)).astype(np.float32)
+    t = rng.normal(0, 0.1, (a.samples, 5)).astype(np.float32)
+    m = MLP(seed=0)
+    m.set_data(f, t)
+    if a.warmup:
+        m.train(a.warmup, a.batch, 1e-3, n_report=1)
+    r = m.train(a.steps, a.batch, 1e-3, n_report=1)
+    flop = 6.0 * a.batch * m.n_param  # forward 2, backward 4 flops per weight and sample
+    ms = float(r["ms"]) / a.steps
+    print(json.dumps({"batch": a.batch, "steps": a.steps, "ms_per_step": round(ms, 4),
+                      "tflops": round(flop / (ms * 1e-3) / 1e12, 2), "loss": float(r["loss"][-1])}))
+    m.close()
+
+
+if __name__ == "__main__":
+    main()
