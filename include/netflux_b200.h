@@ -257,14 +257,37 @@ int nf_step(nf_solver* s);
 int nf_stage(nf_solver* s, int stage);
 /* Halo exchange of a mesh split across solvers (one per part, each part with
  * two layers of halo cells; netflux_b200/partition.py builds the parts and
- * the exchange plan): nf_halo_pack gathers the primitives the next stage
- * reads, of the n cells listed (device numbering, int64 on the device), into
- * the device buffer buf [5][n]; nf_halo_unpack writes such a buffer into the
- * listed cells. Both run on the solver's stream and return when done. No
- * counterpart in the reference (its MPI decomposition is a commented-out
- * sketch, Decomposition.cpp:3-51). */
+ * the exchange plan): nf_halo_pack gathers what the next stage (nf_stage)
+ * reads of the n cells listed (device numbering, int64 on the device) into
+ * the device buffer buf [10][n]: rows 0-4 the primitives, rows 5-9 the
+ * conserved stage input (U, or the RK stage for stages 1 and 2);
+ * nf_halo_unpack writes such a buffer into the listed cells. Both run on the
+ * solver's stream and return when done. No counterpart in the reference (its
+ * MPI decomposition is a commented-out sketch, Decomposition.cpp:3-51). */
 int nf_halo_pack(nf_solver* s, const int64_t* cells, int64_t n, double* buf);
 int nf_halo_unpack(nf_solver* s, const int64_t* cells, int64_t n, const double* buf);
+/* The same split stepped on the device without host waits: nf_split_create
+ * takes the parts' solvers (same parameters; each on its own device or
+ * sharing one; peer access is enabled between their devices), nf_split_link
+ * one direction of the exchange plan (the owner part `from`, the receiving
+ * part `to`, n device cell indices on each side, host arrays).
+ * nf_split_advance queues n steps: each step's dt on every part (with a
+ * global dt, the minimum over the parts, reduced on the device into every
+ * part), then per stage every halo (primitives and conserved stage input)
+ * written by a kernel on the receiver's stream that reads the owner's (its
+ * own GPU, or a peer GPU over NVLink), the parts' streams ordered by events,
+ * then the stage on every part. nf_split_synchronize waits for the parts and returns the first
+ * failing part's status. A part must not be stepped on its own while it is in
+ * a split. NULL from nf_split_create: nf_split_last_error(NULL). No
+ * counterpart in the reference (Decomposition.cpp:3-51 is a commented-out
+ * sketch). */
+typedef struct nf_split nf_split;
+nf_split* nf_split_create(nf_solver* const* parts, int n_parts);
+int nf_split_link(nf_split* sp, int from, int to, const int64_t* from_cells, const int64_t* to_cells, int64_t n);
+int nf_split_advance(nf_split* sp, int64_t n_steps);
+int nf_split_synchronize(nf_split* sp);
+const char* nf_split_last_error(const nf_split* sp);
+void nf_split_destroy(nf_split* sp);
 /* n_steps x (calc_timestep + step) on the device; time (may be NULL) returns
  * the accumulated time. Uses a CUDA graph after the first call. */
 int nf_advance(nf_solver* s, int64_t n_steps, double* time_out);

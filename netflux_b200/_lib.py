@@ -33,7 +33,8 @@ EXPORTED = (
     "nf_mesh_from_su2", "nf_mesh_from_arrays", "nf_mesh_from_arrays_device", "nf_mesh_concat", "nf_mesh_get_info", "nf_mesh_get_patch",
     "nf_mesh_export", "nf_mesh_get_permutation", "nf_mesh_get_case_offsets", "nf_mesh_destroy",
     "nf_params_default", "nf_create", "nf_set_state", "nf_get_state", "nf_set_state_old", "nf_calc_timestep", "nf_set_timestep",
-    "nf_step", "nf_stage", "nf_halo_pack", "nf_halo_unpack", "nf_advance", "nf_get_residual", "nf_get_field", "nf_synchronize", "nf_last_error", "nf_destroy",
+    "nf_step", "nf_stage", "nf_halo_pack", "nf_halo_unpack", "nf_split_create", "nf_split_link", "nf_split_advance",
+    "nf_split_synchronize", "nf_split_last_error", "nf_split_destroy", "nf_advance", "nf_get_residual", "nf_get_field", "nf_synchronize", "nf_last_error", "nf_destroy",
     "nf_time_steps", "nf_residual_norms_noalloc", "nf_tune", "nf_set_launch_shapes", "nf_snapshot_begin", "nf_snapshot_wait", "nf_upload_begin", "nf_upload_commit", "nf_upload_wait", "nf_solve_steady", "nf_solve_steady_to", "nf_fastmath_selftest", "nf_check_mesh_size", "nf_set_host_threads",
     "nf_mlp_param_count", "nf_mlp_create", "nf_mlp_last_error", "nf_mlp_destroy", "nf_mlp_get_params",
     "nf_mlp_set_params", "nf_mlp_set_data", "nf_mlp_train", "nf_mlp_gradients", "nf_mlp_predict",
@@ -106,6 +107,12 @@ def load() -> C.CDLL:
         "nf_stage": (I, [P, I]),
         "nf_halo_pack": (I, [P, P, I64, P]),
         "nf_halo_unpack": (I, [P, P, I64, P]),
+        "nf_split_create": (P, [C.POINTER(P), I]),
+        "nf_split_link": (I, [P, I, I, i64p, i64p, I64]),
+        "nf_split_advance": (I, [P, I64]),
+        "nf_split_synchronize": (I, [P]),
+        "nf_split_last_error": (C.c_char_p, [P]),
+        "nf_split_destroy": (None, [P]),
         "nf_advance": (I, [P, I64, dp]),
         "nf_get_residual": (I, [P, dp, I]),
         "nf_get_field": (I, [P, I, dp, I64]),

@@ -3,16 +3,20 @@
 // 4 hidden layers of 128 SiLU units -> 5 outputs (conserved variables
 // normalised by the free stream). BF16 weights and activations, FP32
 // accumulation in tensor memory, hand-written tcgen05 kernels:
-//   mlp_forward_kernel     all five layers of a 128-sample tile in one CTA,
-//                          weights resident in shared memory, the TMEM
-//                          accumulator turned into the next layer's operand by
-//                          the SiLU epilogue; optionally saves activations and
-//                          the loss gradient
+//   mlp_forward_kernel     all five layers of a 128-sample tile, weights
+//                          resident in shared memory, the TMEM accumulator
+//                          turned into the next layer's operand by the SiLU
+//                          epilogue; two tiles in flight per CTA (one
+//                          warpgroup, operand buffer and accumulator each), so
+//                          one tile's MMAs overlap the other's epilogue;
+//                          optionally saves activations and the loss gradient
 //   mlp_backward_kernel    the same structure backwards (transposed weights,
 //                          SiLU derivative in the epilogue) -> dZ of each layer
 //   mlp_wgrad_kernel       dW = dZ^T H over the batch (split over CTAs), batch
-//                          tiles transposed while staged, five accumulators in
-//                          TMEM, bias gradients through a column of ones
+//                          chunks transposed while staged into one of two
+//                          operand buffers as the other's MMAs run, five
+//                          accumulators in TMEM, bias gradients through a
+//                          column of ones
 //   mlp_adam_kernel        sums the per-CTA partial gradients, Adam update of
 //                          the FP32 master weights, BF16 operand images
 // Parameters in FP32 (padded shapes): W0 [128][16] (inputs 0..6, bias in
@@ -43,7 +47,7 @@ constexpr int NOUT = 16;  // 5 outputs and padding
 constexpr int NIN = 7;
 constexpr int NO = 5;
 constexpr int TILE = 128;  // samples per tile (MMA M)
-constexpr int KC = 64;     // batch rows per weight-gradient chunk
+constexpr int KC = 32;     // batch rows per weight-gradient chunk
 constexpr int NAUG = H + 16;  // H columns, a column of ones, padding
 constexpr long long kWaitCycles = 4000000000LL;  // about 2 s
 
@@ -106,25 +110,52 @@ __device__ __forceinline__ void unpack8(uint4 r, float* v) {
   }
 }
 
+// Tiles in flight per CTA in the forward and backward kernels: each has its
+// own 128 threads (one warpgroup), operand buffers, mbarrier and TMEM
+// accumulator, so one tile's MMAs run while another's epilogue does.
+constexpr int NSLOT = 2;
+// CTAs that give every slot at least one tile of B samples
+inline int tile_ctas(int64_t B) { return int(((B + TILE - 1) / TILE + NSLOT - 1) / NSLOT); }
+
+// Barrier among the 128 threads of one slot (named barriers 1..NSLOT; 0 is
+// __syncthreads), optionally AND-reducing a predicate over them.
+__device__ __forceinline__ void slot_sync(int slot) { asm volatile("bar.sync %0, 128;" ::"r"(slot + 1) : "memory"); }
+__device__ __forceinline__ bool slot_sync_and(int slot, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t"
+      ".reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.and.pred p, %2, 128, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t"
+      "}\n"
+      : "=r"(r)
+      : "r"(uint32_t(v)), "r"(slot + 1)
+      : "memory");
+  return r != 0;
+}
+
 struct TileSync {
   uint32_t mbar;
   uint32_t phase = 0;
   unsigned* status;
-  // wait for the MMAs committed to mbar; every thread agrees on the outcome
+  int slot = -1;  // -1: the whole CTA takes part; else the slot's 128 threads
+  // wait for the MMAs committed to mbar; every participating thread agrees on
+  // the outcome
   __device__ bool wait() {
     const bool ok = umma::mbar_wait(mbar, phase, kWaitCycles);
     phase ^= 1u;
-    const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
-    if (!all_ok && threadIdx.x == 0) atomicOr(status, 1u);
+    const bool all_ok = slot < 0 ? __syncthreads_and(ok ? 1 : 0) != 0 : slot_sync_and(slot, ok);
+    if (!all_ok && (threadIdx.x & 127) == 0) atomicOr(status, 1u);
     umma::fence_after_sync();
     return all_ok;
   }
 };
 
-// Common prologue: mbarrier, TMEM columns; returns the TMEM base address.
-__device__ uint32_t setup(uint64_t* mbar, uint32_t* tslot, uint32_t ncols) {
+// Common prologue: n mbarriers, TMEM columns; returns the TMEM base address.
+__device__ uint32_t setup(uint64_t* mbar, int n, uint32_t* tslot, uint32_t ncols) {
   if (threadIdx.x == 0) {
-    umma::mbar_init(umma::smem_addr(mbar), 1);
+    for (int i = 0; i < n; i++) umma::mbar_init(umma::smem_addr(mbar + i), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (threadIdx.x < 32) umma::tmem_alloc(umma::smem_addr(tslot), ncols);
@@ -158,32 +189,34 @@ struct FwdArgs {
   unsigned* status;
 };
 
-constexpr int FWD_SMEM = IMG_FWD + TILE * H * 2 + TILE * KIN * 2 + (3 * H + NOUT) * 4 + 64;
+constexpr int FWD_SLOT = TILE * H * 2 + TILE * KIN * 2;  // one tile's activations and inputs
+constexpr int FWD_SMEM = IMG_FWD + NSLOT * FWD_SLOT + (3 * H + NOUT) * 4 + 64;
 
-__global__ void __launch_bounds__(128, 1) mlp_forward_kernel(FwdArgs a) {
+__global__ void __launch_bounds__(128 * NSLOT, 1) mlp_forward_kernel(FwdArgs a) {
   extern __shared__ __align__(1024) uint8_t sm[];
+  const int slot = threadIdx.x >> 7, t = threadIdx.x & 127, w = t >> 5;
   uint8_t* s_img = sm;
-  uint8_t* s_act = sm + IMG_FWD;                 // [128 x K128] activations
-  uint8_t* s_x0 = s_act + TILE * H * 2;          // [128 x K16] inputs
-  float* s_bias = reinterpret_cast<float*>(s_x0 + TILE * KIN * 2);  // b1, b2, b3, b4
-  uint64_t* s_mbar = reinterpret_cast<uint64_t*>(s_bias + 3 * H + NOUT);
-  uint32_t* s_tslot = reinterpret_cast<uint32_t*>(s_mbar + 1);
-  const int t = threadIdx.x, w = t >> 5;
+  uint8_t* s_act = sm + IMG_FWD + slot * FWD_SLOT;  // [128 x K128] activations of this slot's tile
+  uint8_t* s_x0 = s_act + TILE * H * 2;             // [128 x K16] inputs
+  float* s_bias = reinterpret_cast<float*>(sm + IMG_FWD + NSLOT * FWD_SLOT);  // b1, b2, b3, b4
+  uint64_t* s_mbar = reinterpret_cast<uint64_t*>(s_bias + 3 * H + NOUT);    // one per slot
+  uint32_t* s_tslot = reinterpret_cast<uint32_t*>(s_mbar + NSLOT);
   {
     const uint4* src = reinterpret_cast<const uint4*>(a.img);
     uint4* dst = reinterpret_cast<uint4*>(s_img);
-    for (int i = t; i < IMG_FWD / 16; i += blockDim.x) dst[i] = src[i];
-    for (int i = t; i < 3 * H + NOUT; i += blockDim.x)
+    for (int i = threadIdx.x; i < IMG_FWD / 16; i += blockDim.x) dst[i] = src[i];
+    for (int i = threadIdx.x; i < 3 * H + NOUT; i += blockDim.x)
       s_bias[i] = i < 3 * H ? a.params[OFF_B1 + i] : a.params[OFF_B4 + i - 3 * H];
   }
-  const uint32_t tbase = setup(s_mbar, s_tslot, 128);
-  TileSync sync{umma::smem_addr(s_mbar), 0u, a.status};
-  const uint32_t lane_addr = tbase + (uint32_t(w * 32) << 16);
+  const uint32_t tbase = setup(s_mbar, NSLOT, s_tslot, 128 * NSLOT);
+  TileSync sync{umma::smem_addr(s_mbar + slot), 0u, a.status, slot};
+  const uint32_t tacc = tbase + uint32_t(slot * 128);  // this slot's 128 accumulator columns
+  const uint32_t lane_addr = tacc + (uint32_t(w * 32) << 16);
   const uint32_t a_act = umma::smem_addr(s_act), a_x0 = umma::smem_addr(s_x0), a_img = umma::smem_addr(s_img);
   const uint32_t id128 = umma::idesc_bf16(128, 128), id16 = umma::idesc_bf16(128, 16);
   const int64_t n_tiles = (a.B + TILE - 1) / TILE;
   float ssq = 0.f;
-  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+  for (int64_t tile = int64_t(blockIdx.x) * NSLOT + slot; tile < n_tiles; tile += int64_t(gridDim.x) * NSLOT) {
     const int64_t b = tile * TILE + t;
     const bool valid = b < a.B;
     {  // inputs: 7 features, a constant 1 (bias of layer 0), zeros
@@ -206,17 +239,17 @@ __global__ void __launch_bounds__(128, 1) mlp_forward_kernel(FwdArgs a) {
       }
     }
     umma::fence_async_shared();
-    __syncthreads();
+    slot_sync(slot);
     for (int l = 0; l < 5; l++) {
       if (t == 0) {
         umma::fence_after_sync();
         if (l == 0) {
-          umma::mma_bf16(tbase, umma::kmaj_desc(a_x0, KIN, 0), umma::kmaj_desc(a_img + IMG_W0, KIN, 0), id128, 0);
+          umma::mma_bf16(tacc, umma::kmaj_desc(a_x0, KIN, 0), umma::kmaj_desc(a_img + IMG_W0, KIN, 0), id128, 0);
         } else {
           const int img = l == 1 ? IMG_W1 : l == 2 ? IMG_W2 : l == 3 ? IMG_W3 : IMG_W4;
 #pragma unroll 1
           for (int s = 0; s < H / 16; s++)
-            umma::mma_bf16(tbase, umma::kmaj_desc(a_act, H, s), umma::kmaj_desc(a_img + img, H, s),
+            umma::mma_bf16(tacc, umma::kmaj_desc(a_act, H, s), umma::kmaj_desc(a_img + img, H, s),
                            l == 4 ? id16 : id128, s > 0 ? 1u : 0u);
         }
         umma::commit(sync.mbar);
@@ -276,7 +309,7 @@ __global__ void __launch_bounds__(128, 1) mlp_forward_kernel(FwdArgs a) {
       // TMEM read and operand written before the next MMA
       umma::fence_before_sync();
       umma::fence_async_shared();
-      __syncthreads();
+      slot_sync(slot);
     }
   }
 done:
@@ -285,7 +318,7 @@ done:
     for (int off = 16; off > 0; off >>= 1) ssq += __shfl_xor_sync(0xffffffffu, ssq, off);
     if ((t & 31) == 0 && ssq != 0.f) atomicAdd(a.loss, double(ssq));
   }
-  teardown(tbase, 128);
+  teardown(tbase, 128 * NSLOT);
 }
 
 // ---------------------------------------------------------------------------
@@ -300,28 +333,30 @@ struct BwdArgs {
   unsigned* status;
 };
 
-constexpr int BWD_SMEM = IMG_BWD + TILE * H * 2 + TILE * NOUT * 2 + 64;
+constexpr int BWD_SLOT = TILE * H * 2 + TILE * NOUT * 2;  // one tile's operand and output gradient
+constexpr int BWD_SMEM = IMG_BWD + NSLOT * BWD_SLOT + 64;
 
-__global__ void __launch_bounds__(128, 1) mlp_backward_kernel(BwdArgs a) {
+__global__ void __launch_bounds__(128 * NSLOT, 1) mlp_backward_kernel(BwdArgs a) {
   extern __shared__ __align__(1024) uint8_t sm[];
+  const int slot = threadIdx.x >> 7, t = threadIdx.x & 127, w = t >> 5;
   uint8_t* s_img = sm;
-  uint8_t* s_act = sm + IMG_BWD;
+  uint8_t* s_act = sm + IMG_BWD + slot * BWD_SLOT;
   uint8_t* s_d4 = s_act + TILE * H * 2;
-  uint64_t* s_mbar = reinterpret_cast<uint64_t*>(s_d4 + TILE * NOUT * 2);
-  uint32_t* s_tslot = reinterpret_cast<uint32_t*>(s_mbar + 1);
-  const int t = threadIdx.x, w = t >> 5;
+  uint64_t* s_mbar = reinterpret_cast<uint64_t*>(sm + IMG_BWD + NSLOT * BWD_SLOT);  // one per slot
+  uint32_t* s_tslot = reinterpret_cast<uint32_t*>(s_mbar + NSLOT);
   {
     const uint4* src = reinterpret_cast<const uint4*>(a.img);
     uint4* dst = reinterpret_cast<uint4*>(s_img);
-    for (int i = t; i < IMG_BWD / 16; i += blockDim.x) dst[i] = src[i];
+    for (int i = threadIdx.x; i < IMG_BWD / 16; i += blockDim.x) dst[i] = src[i];
   }
-  const uint32_t tbase = setup(s_mbar, s_tslot, 128);
-  TileSync sync{umma::smem_addr(s_mbar), 0u, a.status};
-  const uint32_t lane_addr = tbase + (uint32_t(w * 32) << 16);
+  const uint32_t tbase = setup(s_mbar, NSLOT, s_tslot, 128 * NSLOT);
+  TileSync sync{umma::smem_addr(s_mbar + slot), 0u, a.status, slot};
+  const uint32_t tacc = tbase + uint32_t(slot * 128);  // this slot's 128 accumulator columns
+  const uint32_t lane_addr = tacc + (uint32_t(w * 32) << 16);
   const uint32_t a_act = umma::smem_addr(s_act), a_d4 = umma::smem_addr(s_d4), a_img = umma::smem_addr(s_img);
   const uint32_t id128 = umma::idesc_bf16(128, 128);
   const int64_t n_tiles = (a.B + TILE - 1) / TILE;
-  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+  for (int64_t tile = int64_t(blockIdx.x) * NSLOT + slot; tile < n_tiles; tile += int64_t(gridDim.x) * NSLOT) {
     const int64_t b = tile * TILE + t;
     const bool valid = b < a.B;
     {
@@ -335,18 +370,18 @@ __global__ void __launch_bounds__(128, 1) mlp_backward_kernel(BwdArgs a) {
       *reinterpret_cast<uint4*>(s_d4 + umma::kmaj_off(t, 8, NOUT)) = c1;
     }
     umma::fence_async_shared();
-    __syncthreads();
+    slot_sync(slot);
     // layer l's input gradient: dH_{l-1} = dZ_l W_l, then dZ_{l-1} = dH_{l-1} silu'(Z_{l-1})
     for (int l = 4; l >= 1; l--) {
       if (t == 0) {
         umma::fence_after_sync();
         if (l == 4) {
-          umma::mma_bf16(tbase, umma::kmaj_desc(a_d4, NOUT, 0), umma::kmaj_desc(a_img + IMG_T4, NOUT, 0), id128, 0);
+          umma::mma_bf16(tacc, umma::kmaj_desc(a_d4, NOUT, 0), umma::kmaj_desc(a_img + IMG_T4, NOUT, 0), id128, 0);
         } else {
           const int img = l == 1 ? IMG_T1 : l == 2 ? IMG_T2 : IMG_T3;
 #pragma unroll 1
           for (int s = 0; s < H / 16; s++)
-            umma::mma_bf16(tbase, umma::kmaj_desc(a_act, H, s), umma::kmaj_desc(a_img + img, H, s), id128,
+            umma::mma_bf16(tacc, umma::kmaj_desc(a_act, H, s), umma::kmaj_desc(a_img + img, H, s), id128,
                            s > 0 ? 1u : 0u);
         }
         umma::commit(sync.mbar);
@@ -384,11 +419,11 @@ __global__ void __launch_bounds__(128, 1) mlp_backward_kernel(BwdArgs a) {
       }
       umma::fence_before_sync();
       umma::fence_async_shared();
-      __syncthreads();
+      slot_sync(slot);
     }
   }
 done:
-  teardown(tbase, 128);
+  teardown(tbase, 128 * NSLOT);
 }
 
 // ---------------------------------------------------------------------------
@@ -403,10 +438,12 @@ struct WgArgs {
   unsigned* status;
 };
 
-constexpr int WG_A = H * KC * 2;      // one [128 x K64] operand
-constexpr int WG_BA = NAUG * KC * 2;  // one [144 x K64] operand
-constexpr int WG_B16 = 16 * KC * 2;   // one [16 x K64] operand
-constexpr int WG_SMEM = 5 * WG_A + 3 * WG_BA + 2 * WG_B16 + 64;
+constexpr int WG_A = H * KC * 2;      // one [128 x KC] operand
+constexpr int WG_BA = NAUG * KC * 2;  // one [144 x KC] operand
+constexpr int WG_B16 = 16 * KC * 2;   // one [16 x KC] operand
+constexpr int WG_BUF = 5 * WG_A + 3 * WG_BA + 2 * WG_B16;  // one chunk's operands
+constexpr int WG_THREADS = 256;
+constexpr int WG_SMEM = 2 * WG_BUF + 64;  // two chunks: one staged while the other's MMAs run
 // TMEM columns of the five accumulators (32-column aligned; 512 allocated)
 constexpr int ACC1 = 0, ACC2 = 160, ACC3 = 320, ACC0 = 480, ACC4 = 496;
 
@@ -425,7 +462,7 @@ __device__ __forceinline__ uint4 column8(const uint4 v[8], int q) {
   return o;
 }
 
-// rows [0, F) of a K-major [rows x K64] tile <- transpose of a [KC][F] row-major
+// rows [0, F) of a K-major [rows x KC] tile <- transpose of a [KC][F] row-major
 // BF16 block (batch rows b0 .. b0+KC; rows past B are zero). Each task is one
 // 8-feature chunk of 8 consecutive batch rows: eight 16-byte loads, an 8 x 8
 // transpose in registers, eight 16-byte stores of core-matrix rows.
@@ -452,75 +489,103 @@ __device__ __forceinline__ void stage_t16(uint8_t* dst, const __nv_bfloat16* src
   stage_t<16>(dst, src, b0, B);
 }
 
-__global__ void __launch_bounds__(128, 1) mlp_wgrad_kernel(WgArgs a) {
-  extern __shared__ __align__(1024) uint8_t sm[];
-  uint8_t* sA[5];  // dZ0^T, dZ1^T, dZ2^T, dZ3^T, H3^T
-  for (int i = 0; i < 5; i++) sA[i] = sm + i * WG_A;
-  uint8_t* sB[3];  // [H0|1]^T, [H1|1]^T, [H2|1]^T
-  for (int i = 0; i < 3; i++) sB[i] = sm + 5 * WG_A + i * WG_BA;
-  uint8_t* sX = sm + 5 * WG_A + 3 * WG_BA;  // X0^T
-  uint8_t* sD4 = sX + WG_B16;                // dZ4^T
-  uint64_t* s_mbar = reinterpret_cast<uint64_t*>(sD4 + WG_B16);
-  uint32_t* s_tslot = reinterpret_cast<uint32_t*>(s_mbar + 1);
-  const int t = threadIdx.x, w = t >> 5;
-  // constant rows of the augmented operands: a row of ones, then zeros
-  for (int i = 0; i < 3; i++)
-    for (int r = H + t / 8; r < NAUG; r += 16) {
-      float v[8];
-      const int g = t % 8;
+struct WgBuf {
+  uint8_t* A[5];  // dZ0^T, dZ1^T, dZ2^T, dZ3^T, H3^T
+  uint8_t* B[3];  // [H0|1]^T, [H1|1]^T, [H2|1]^T
+  uint8_t* X;     // X0^T
+  uint8_t* D4;    // dZ4^T
+  __device__ explicit WgBuf(uint8_t* base) {
+    for (int i = 0; i < 5; i++) A[i] = base + i * WG_A;
+    for (int i = 0; i < 3; i++) B[i] = base + 5 * WG_A + i * WG_BA;
+    X = base + 5 * WG_A + 3 * WG_BA;
+    D4 = X + WG_B16;
+  }
+  // the chunk of KC batch rows from b0, transposed into K-major operands
+  __device__ void stage(const WgArgs& a, int64_t b0) {
 #pragma unroll
-      for (int j = 0; j < 8; j++) v[j] = r == H ? 1.f : 0.f;
-      *reinterpret_cast<uint4*>(sB[i] + umma::kmaj_off(r, g * 8, KC)) = pack8(v);
+    for (int l = 0; l < 4; l++) stage_t128(A[l], a.dz + int64_t(l) * a.B * H, b0, a.B);
+    stage_t128(A[4], a.save + save_h(a.B, 3), b0, a.B);
+#pragma unroll
+    for (int l = 0; l < 3; l++) stage_t128(B[l], a.save + save_h(a.B, l), b0, a.B);
+    stage_t16(X, a.save + save_x0(a.B), b0, a.B);
+    stage_t16(D4, a.dz4, b0, a.B);
+  }
+  // every accumulator += this chunk's product (one thread)
+  __device__ void issue(uint32_t tbase, bool first) const {
+    const uint32_t idA = umma::idesc_bf16(128, NAUG), id16 = umma::idesc_bf16(128, 16);
+#pragma unroll 1
+    for (int s = 0; s < KC / 16; s++) {
+      const uint32_t acc = (first && s == 0) ? 0u : 1u;
+#pragma unroll
+      for (int l = 1; l <= 3; l++)
+        umma::mma_bf16(tbase + uint32_t(l == 1 ? ACC1 : l == 2 ? ACC2 : ACC3),
+                       umma::kmaj_desc(umma::smem_addr(A[l]), KC, s), umma::kmaj_desc(umma::smem_addr(B[l - 1]), KC, s),
+                       idA, acc);
+      umma::mma_bf16(tbase + ACC0, umma::kmaj_desc(umma::smem_addr(A[0]), KC, s),
+                     umma::kmaj_desc(umma::smem_addr(X), KC, s), id16, acc);
+      umma::mma_bf16(tbase + ACC4, umma::kmaj_desc(umma::smem_addr(A[4]), KC, s),
+                     umma::kmaj_desc(umma::smem_addr(D4), KC, s), id16, acc);
     }
-  const uint32_t tbase = setup(s_mbar, s_tslot, 512);
-  TileSync sync{umma::smem_addr(s_mbar), 0u, a.status};
-  const uint32_t idA = umma::idesc_bf16(128, NAUG), id16 = umma::idesc_bf16(128, 16);
+  }
+};
+
+// The CTA's chunks in turn through two operand buffers: while the tensor core
+// multiplies chunk i from one buffer, the threads stage chunk i + 1 into the
+// other (after the MMAs of chunk i - 1, which read it, are done).
+__global__ void __launch_bounds__(WG_THREADS, 1) mlp_wgrad_kernel(WgArgs a) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  uint64_t* s_mbar = reinterpret_cast<uint64_t*>(sm + 2 * WG_BUF);  // one per buffer
+  uint32_t* s_tslot = reinterpret_cast<uint32_t*>(s_mbar + 2);
+  const int t = threadIdx.x;
+  // constant rows of the augmented operands: a row of ones, then zeros
+  for (int task = t; task < 2 * 3 * (NAUG - H) * (KC / 8); task += blockDim.x) {
+    const int g = task % (KC / 8), r = H + (task / (KC / 8)) % (NAUG - H), i = task / (KC / 8) / (NAUG - H);
+    float v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) v[j] = r == H ? 1.f : 0.f;
+    uint8_t* op = sm + (i / 3) * WG_BUF + 5 * WG_A + (i % 3) * WG_BA;  // WgBuf::B[i % 3] of buffer i / 3
+    *reinterpret_cast<uint4*>(op + umma::kmaj_off(r, g * 8, KC)) = pack8(v);
+  }
+  const uint32_t tbase = setup(s_mbar, 2, s_tslot, 512);
+  TileSync sync0{umma::smem_addr(s_mbar), 0u, a.status}, sync1{umma::smem_addr(s_mbar + 1), 0u, a.status};
+  auto wait_buf = [&](int k) { return k == 0 ? sync0.wait() : sync1.wait(); };
   const int64_t n_chunks = (a.B + KC - 1) / KC;
   float db4 = 0.f;
-  bool first = true;
-  for (int64_t ch = blockIdx.x; ch < n_chunks; ch += gridDim.x) {
-    const int64_t b0 = ch * KC;
-    for (int l = 0; l < 4; l++) stage_t128(sA[l], a.dz + int64_t(l) * a.B * H, b0, a.B);
-    stage_t128(sA[4], a.save + save_h(a.B, 3), b0, a.B);
-    for (int l = 0; l < 3; l++) stage_t128(sB[l], a.save + save_h(a.B, l), b0, a.B);
-    stage_t16(sX, a.save + save_x0(a.B), b0, a.B);
-    stage_t16(sD4, a.dz4, b0, a.B);
-    if (t < 16)
-      for (int j = 0; j < KC; j++) {
-        const int64_t b = b0 + j;
-        if (b < a.B) db4 += __bfloat162float(a.dz4[b * 16 + t]);
-      }
-    umma::fence_async_shared();
-    __syncthreads();
+  int i = 0;  // chunks of this CTA issued
+  if (int64_t(blockIdx.x) < n_chunks) WgBuf(sm).stage(a, int64_t(blockIdx.x) * KC);
+  umma::fence_async_shared();
+  __syncthreads();
+  for (int64_t ch = blockIdx.x; ch < n_chunks; ch += gridDim.x, i++) {
+    const int cur = i & 1;
     if (t == 0) {
       umma::fence_after_sync();
-#pragma unroll 1
-      for (int s = 0; s < KC / 16; s++) {
-        const uint32_t acc = (first && s == 0) ? 0u : 1u;
-        for (int l = 1; l <= 3; l++)
-          umma::mma_bf16(tbase + uint32_t(l == 1 ? ACC1 : l == 2 ? ACC2 : ACC3),
-                         umma::kmaj_desc(umma::smem_addr(sA[l]), KC, s),
-                         umma::kmaj_desc(umma::smem_addr(sB[l - 1]), KC, s), idA, acc);
-        umma::mma_bf16(tbase + ACC0, umma::kmaj_desc(umma::smem_addr(sA[0]), KC, s),
-                       umma::kmaj_desc(umma::smem_addr(sX), KC, s), id16, acc);
-        umma::mma_bf16(tbase + ACC4, umma::kmaj_desc(umma::smem_addr(sA[4]), KC, s),
-                       umma::kmaj_desc(umma::smem_addr(sD4), KC, s), id16, acc);
-      }
-      umma::commit(sync.mbar);
+      WgBuf(sm + cur * WG_BUF).issue(tbase, i == 0);
+      umma::commit(cur == 0 ? sync0.mbar : sync1.mbar);
     }
-    first = false;
-    if (!sync.wait()) goto done;
-    umma::fence_before_sync();
-    __syncthreads();  // operands consumed before the next chunk overwrites them
+    // bias gradient of the output layer: this thread's output t & 15 over the chunk's rows
+    // t >> 4 and (t >> 4) + 16 (two independent loads, no thread waits on a serial sum)
+#pragma unroll
+    for (int j = t >> 4; j < KC; j += WG_THREADS / 16) {
+      const int64_t b = ch * KC + j;
+      if (b < a.B) db4 += __bfloat162float(a.dz4[b * 16 + (t & 15)]);
+    }
+    const int64_t nx = ch + gridDim.x;
+    if (nx < n_chunks) {
+      if (i >= 1 && !wait_buf(cur ^ 1)) goto done;  // chunk i - 1 has read the other buffer
+      WgBuf(sm + (cur ^ 1) * WG_BUF).stage(a, nx * KC);
+      umma::fence_async_shared();
+    }
+    __syncthreads();  // the next chunk's operands staged before it is issued
   }
+  if (i > 0 && !wait_buf((i - 1) & 1)) goto done;  // the last chunk, and with it every earlier one
   {
     float* P = a.partial + int64_t(blockIdx.x) * N_PARAM;
-    const int row = t;  // TMEM lane of this thread
-    const uint32_t lane_addr = tbase + (uint32_t(w * 32) << 16);
-    if (first) {  // this CTA had no rows
-      for (int i = t; i < N_PARAM; i += blockDim.x) P[i] = 0.f;
+    const int row = t & 127, half = t >> 7;  // TMEM lane; which accumulators this warpgroup reads
+    const uint32_t lane_addr = tbase + (uint32_t(((t >> 5) & 3) * 32) << 16);
+    if (i == 0) {  // this CTA had no rows
+      for (int k = t; k < N_PARAM; k += blockDim.x) P[k] = 0.f;
     } else {
-      for (int l = 1; l <= 3; l++) {
+      for (int l = 1 + half; l <= 3; l += 2) {  // layers 1, 3 | 2
         const uint32_t base = lane_addr + uint32_t(l == 1 ? ACC1 : l == 2 ? ACC2 : ACC3);
         const int offW = l == 1 ? OFF_W1 : l == 2 ? OFF_W2 : OFF_W3;
         const int offB = l == 1 ? OFF_B1 : l == 2 ? OFF_B2 : OFF_B3;
@@ -535,14 +600,26 @@ __global__ void __launch_bounds__(128, 1) mlp_wgrad_kernel(WgArgs a) {
         umma::tmem_ld16(base + uint32_t(H), v);
         P[offB + row] = v[0];
       }
-      float v[16];
-      umma::tmem_ld16(lane_addr + ACC0, v);
+      if (half == 1) {
+        float v[16];
+        umma::tmem_ld16(lane_addr + ACC0, v);
 #pragma unroll
-      for (int j = 0; j < 16; j++) P[OFF_W0 + row * KIN + j] = v[j];
-      umma::tmem_ld16(lane_addr + ACC4, v);
+        for (int j = 0; j < 16; j++) P[OFF_W0 + row * KIN + j] = v[j];
+        umma::tmem_ld16(lane_addr + ACC4, v);
 #pragma unroll
-      for (int j = 0; j < 16; j++) P[OFF_W4 + j * H + row] = v[j];
-      if (t < 16) P[OFF_B4 + t] = db4;
+        for (int j = 0; j < 16; j++) P[OFF_W4 + j * H + row] = v[j];
+      }
+      // db4: the two lanes of a warp with the same output, then the warps in order
+      // (a fixed order: the same bits every run); the operand buffers are free now
+      db4 += __shfl_xor_sync(0xffffffffu, db4, 16);
+      float* s_db4 = reinterpret_cast<float*>(sm);  // [warps][16]
+      if ((t & 31) < 16) s_db4[(t >> 5) * 16 + (t & 15)] = db4;
+      __syncthreads();
+      if (t < 16) {
+        float sum = 0.f;
+        for (int wq = 0; wq < WG_THREADS / 32; wq++) sum += s_db4[wq * 16 + t];
+        P[OFF_B4 + t] = sum;
+      }
     }
   }
 done:
@@ -640,7 +717,7 @@ __global__ void __launch_bounds__(128, 1) umma_gemm_test_kernel(const __nv_bfloa
     *reinterpret_cast<__nv_bfloat16*>(sa + umma::kmaj_off(i / K, i % K, K)) = A[i];
   for (int i = t; i < N * K; i += blockDim.x)
     *reinterpret_cast<__nv_bfloat16*>(sb + umma::kmaj_off(i / K, i % K, K)) = B[i];
-  const uint32_t tbase = setup(s_mbar, s_tslot, 256);
+  const uint32_t tbase = setup(s_mbar, 1, s_tslot, 256);
   TileSync sync{umma::smem_addr(s_mbar), 0u, status};
   umma::fence_async_shared();
   __syncthreads();
@@ -783,12 +860,12 @@ struct nf_mlp {
     fa.loss = loss.p;
     fa.loss_scale = 2.0f / float(B * NO);
     fa.status = status.p;
-    const int n_tiles = int((B + TILE - 1) / TILE);
-    mlp_forward_kernel<<<std::min(n_tiles, n_sm), 128, FWD_SMEM, stream>>>(fa);
+    const int n_cta = std::min(tile_ctas(B), n_sm);
+    mlp_forward_kernel<<<n_cta, 128 * NSLOT, FWD_SMEM, stream>>>(fa);
     BwdArgs ba{img_bwd.p, save.p, dz4.p, B, dz.p, status.p};
-    mlp_backward_kernel<<<std::min(n_tiles, n_sm), 128, BWD_SMEM, stream>>>(ba);
+    mlp_backward_kernel<<<n_cta, 128 * NSLOT, BWD_SMEM, stream>>>(ba);
     WgArgs wa{save.p, dz.p, dz4.p, B, partial.p, status.p};
-    mlp_wgrad_kernel<<<n_wg, 128, WG_SMEM, stream>>>(wa);
+    mlp_wgrad_kernel<<<n_wg, WG_THREADS, WG_SMEM, stream>>>(wa);
     mlp_adam_kernel<<<(N_PARAM + 255) / 256, 256, 0, stream>>>(adam_args(lr, apply));
   }
   void check_status() {
@@ -1012,8 +1089,7 @@ int nf_mlp_predict(nf_mlp* m, const float* features, int64_t n, float* out, doub
     ck(cudaEventCreate(&e0), "event");
     ck(cudaEventCreate(&e1), "event");
     ck(cudaEventRecord(e0, m->stream), "event");
-    const int n_tiles = int((n + TILE - 1) / TILE);
-    mlp_forward_kernel<<<std::min(n_tiles, m->n_sm), 128, FWD_SMEM, m->stream>>>(fa);
+    mlp_forward_kernel<<<std::min(tile_ctas(n), m->n_sm), 128 * NSLOT, FWD_SMEM, m->stream>>>(fa);
     ck(cudaGetLastError(), "launch");
     ck(cudaEventRecord(e1, m->stream), "event");
     ck(cudaMemcpyAsync(out, o.p, size_t(n) * NO * sizeof(float), cudaMemcpyDeviceToHost, m->stream), "D2H");

@@ -141,21 +141,59 @@ __global__ void residual_finalize_kernel(const double* __restrict__ part, const 
 
 // Halo exchange of a mesh split across solvers: the stage-input primitives of
 // listed cells (device order) gathered into / scattered from [5][n] rows.
+// Halo rows of a mesh split across solvers: the primitives V and the conserved
+// state U the next stage reads (its stage input; the stage update of a halo
+// cell starts from it), 10 rows of [n] in buf.
 __global__ void halo_pack_kernel(int64_t n, int st, const int64_t* __restrict__ cells, const double* __restrict__ V,
-                                 double* __restrict__ buf) {
+                                 const double* __restrict__ U, double* __restrict__ buf) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int64_t c = cells[i];
 #pragma unroll
-  for (int k = 0; k < 5; k++) buf[k * n + i] = V[size_t(k) * st + c];
+  for (int k = 0; k < 5; k++) {
+    buf[k * n + i] = V[size_t(k) * st + c];
+    buf[(5 + k) * n + i] = U[size_t(k) * st + c];
+  }
 }
 __global__ void halo_unpack_kernel(int64_t n, int st, const int64_t* __restrict__ cells,
-                                   const double* __restrict__ buf, double* __restrict__ V) {
+                                   const double* __restrict__ buf, double* __restrict__ V, double* __restrict__ U) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int64_t c = cells[i];
 #pragma unroll
-  for (int k = 0; k < 5; k++) V[size_t(k) * st + c] = buf[k * n + i];
+  for (int k = 0; k < 5; k++) {
+    V[size_t(k) * st + c] = buf[k * n + i];
+    U[size_t(k) * st + c] = buf[(5 + k) * n + i];
+  }
+}
+// One link of a split mesh: the receiver's halo rows (V and the stage input U)
+// take the sender's (V_from / U_from on this device or, with peer access, on
+// another GPU: plain loads over NVLink).
+__global__ void halo_copy_kernel(int64_t n, int st_from, const int64_t* __restrict__ from_cells,
+                                 const double* __restrict__ V_from, const double* __restrict__ U_from, int st_to,
+                                 const int64_t* __restrict__ to_cells, double* __restrict__ V_to,
+                                 double* __restrict__ U_to) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t a = from_cells[i], b = to_cells[i];
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    V_to[size_t(k) * st_to + b] = V_from[size_t(k) * st_from + a];
+    U_to[size_t(k) * st_to + b] = U_from[size_t(k) * st_from + a];
+  }
+}
+
+// The global time step of a split mesh: every part's minimum replaced by the
+// minimum over the parts (peer loads and stores across GPUs); a NaN wins, so
+// every part's end-of-step check reports it.
+__global__ void split_dt_min_kernel(double* const* __restrict__ scal, int n_parts) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double m = scal[0][nf::kScalDtMin];
+  for (int i = 1; i < n_parts && !isnan(m); i++) {
+    const double v = scal[i][nf::kScalDtMin];
+    if (isnan(v) || v < m) m = v;
+  }
+  for (int i = 0; i < n_parts; i++) scal[i][nf::kScalDtMin] = m;
 }
 
 // AoS state in reference cell order <-> SoA in device order.
@@ -319,6 +357,9 @@ struct nf_solver {
   }
 
   double* Vbuf(int i) { return i ? V1.p : V0.p; }
+  // the conserved state stage s reads (Solver.cpp:103-133: U, then the RK
+  // stage W)
+  double* stage_input(int s) { return (p.time_scheme == NF_TVD_RK3 && s > 0) ? W.p : U.p; }
   double* dtl(int i) { return i ? dt_local2.p : dt_local.p; }
   // the FP64 form's last stage computes the next step's dt (second order:
   // its gradient kernel reads the primitives the reference's dt reads)
@@ -728,6 +769,123 @@ nf_mesh* wrap_mesh(nf::Mesh&& m) {
 }
 
 }  // namespace
+
+// One mesh split across solvers (partition.py's parts): the owner of every
+// halo cell writes its primitives into the receiving part before each stage,
+// by a kernel on the receiver's stream that reads the owner's buffer (same
+// GPU, or a peer GPU over NVLink with plain loads). Events order the parts'
+// streams; the host waits on nothing inside a step.
+struct nf_split {
+  struct Link {
+    int from = 0, to = 0;
+    int64_t n = 0;
+    DevBuf<int64_t> from_cells, to_cells;  // both on the receiver's device
+  };
+  std::vector<nf_solver*> parts;
+  std::vector<std::unique_ptr<Link>> links;
+  std::vector<cudaEvent_t> ready, copied;  // per part: stage input ready; its incoming halos written
+  cudaEvent_t dt_done = nullptr;           // the global dt written into every part
+  DevBuf<double*> scal_ptrs;               // on part 0's device
+  std::string err;
+  bool global_dt = false;
+
+  void set_dev(int d) { ck(cudaSetDevice(d), "cudaSetDevice"); }
+  // every part's halo rows from their owners, before stage k of every part
+  void exchange(int k) {
+    for (size_t i = 0; i < parts.size(); i++) {
+      set_dev(parts[i]->device);
+      ck(cudaEventRecord(ready[i], parts[i]->stream), "cudaEventRecord");
+    }
+    for (auto& lk : links) {
+      nf_solver* a = parts[size_t(lk->from)];
+      nf_solver* b = parts[size_t(lk->to)];
+      set_dev(b->device);
+      ck(cudaStreamWaitEvent(b->stream, ready[size_t(lk->from)], 0), "cudaStreamWaitEvent");
+      halo_copy_kernel<<<int((lk->n + 255) / 256), 256, 0, b->stream>>>(
+          lk->n, a->stride, lk->from_cells.p, a->Vbuf(a->vcur), a->stage_input(k), b->stride, lk->to_cells.p,
+          b->Vbuf(b->vcur), b->stage_input(k));
+      ck(cudaGetLastError(), "halo copy launch");
+    }
+    for (size_t i = 0; i < parts.size(); i++) {
+      set_dev(parts[i]->device);
+      ck(cudaEventRecord(copied[i], parts[i]->stream), "cudaEventRecord");
+    }
+    // stage k of a sender updates in place what the receivers have just read
+    // (the RK stage W at stage 1, U under explicit Euler): it waits for their
+    // copies
+    for (auto& lk : links) {
+      nf_solver* a = parts[size_t(lk->from)];
+      set_dev(a->device);
+      ck(cudaStreamWaitEvent(a->stream, copied[size_t(lk->to)], 0), "cudaStreamWaitEvent");
+    }
+  }
+  // with a global dt: the minimum over the parts into every part
+  void reduce_dt() {
+    for (size_t i = 0; i < parts.size(); i++) {
+      set_dev(parts[i]->device);
+      ck(cudaEventRecord(ready[i], parts[i]->stream), "cudaEventRecord");
+    }
+    nf_solver* p0 = parts[0];
+    set_dev(p0->device);
+    for (size_t i = 1; i < parts.size(); i++)
+      ck(cudaStreamWaitEvent(p0->stream, ready[i], 0), "cudaStreamWaitEvent");
+    split_dt_min_kernel<<<1, 32, 0, p0->stream>>>(scal_ptrs.p, int(parts.size()));
+    ck(cudaGetLastError(), "dt min launch");
+    ck(cudaEventRecord(dt_done, p0->stream), "cudaEventRecord");
+    for (size_t i = 1; i < parts.size(); i++) {
+      set_dev(parts[i]->device);
+      ck(cudaStreamWaitEvent(parts[i]->stream, dt_done, 0), "cudaStreamWaitEvent");
+    }
+  }
+  void step() {
+    for (nf_solver* s : parts) {
+      set_dev(s->device);
+      s->ratchet_due(1);
+      s->enqueue_dt();
+    }
+    if (global_dt) reduce_dt();
+    const int ns = parts[0]->n_stages();
+    for (int k = 0; k < ns; k++) {
+      exchange(k);
+      for (nf_solver* s : parts) {
+        set_dev(s->device);
+        s->enqueue_stage(k);
+      }
+    }
+    for (nf_solver* s : parts) s->steps_done++;
+  }
+  ~nf_split() {
+    for (size_t i = 0; i < parts.size(); i++) {
+      cudaSetDevice(parts[i]->device);
+      cudaStreamSynchronize(parts[i]->stream);
+    }
+    for (auto e : ready)
+      if (e) cudaEventDestroy(e);
+    for (auto e : copied)
+      if (e) cudaEventDestroy(e);
+    if (dt_done) cudaEventDestroy(dt_done);
+  }
+};
+
+// calls on a split mesh: the device is restored, exceptions become status codes
+template <typename F>
+int split_guarded(nf_split* sp, F&& fn) {
+  if (!sp) return NF_ERR_ARG;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int rc;
+  try {
+    rc = fn();
+  } catch (const CudaError& e) {
+    sp->err = e.what();
+    rc = NF_ERR_CUDA;
+  } catch (const std::exception& e) {
+    sp->err = e.what();
+    rc = NF_ERR_ARG;
+  }
+  cudaSetDevice(dev);
+  return rc;
+}
 
 extern "C" {
 
@@ -1443,7 +1601,8 @@ int nf_halo_pack(nf_solver* s, const int64_t* cells, int64_t n, double* buf) {
   return guarded(s, [&]() -> int {
     int rc = halo_args(s, cells, n, buf, "nf_halo_pack");
     if (rc != NF_OK || n == 0) return rc;
-    halo_pack_kernel<<<int((n + 255) / 256), 256, 0, s->stream>>>(n, s->stride, cells, s->Vbuf(s->vcur), buf);
+    halo_pack_kernel<<<int((n + 255) / 256), 256, 0, s->stream>>>(n, s->stride, cells, s->Vbuf(s->vcur),
+                                                                   s->stage_input(s->stage_next), buf);
     ck(cudaGetLastError(), "halo pack");
     ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
     return NF_OK;
@@ -1454,7 +1613,8 @@ int nf_halo_unpack(nf_solver* s, const int64_t* cells, int64_t n, const double* 
   return guarded(s, [&]() -> int {
     int rc = halo_args(s, cells, n, buf, "nf_halo_unpack");
     if (rc != NF_OK || n == 0) return rc;
-    halo_unpack_kernel<<<int((n + 255) / 256), 256, 0, s->stream>>>(n, s->stride, cells, buf, s->Vbuf(s->vcur));
+    halo_unpack_kernel<<<int((n + 255) / 256), 256, 0, s->stream>>>(n, s->stride, cells, buf, s->Vbuf(s->vcur),
+                                                                     s->stage_input(s->stage_next));
     ck(cudaGetLastError(), "halo unpack");
     ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
     return NF_OK;
@@ -1823,6 +1983,132 @@ void nf_destroy(nf_solver* s) {
   cudaStreamSynchronize(s->stream);
   delete s;
   if (dev != own) cudaSetDevice(dev);
+}
+
+// ---------------------------------------------------------------------------
+// a mesh split across solvers
+// ---------------------------------------------------------------------------
+nf_split* nf_split_create(nf_solver* const* parts, int n_parts) {
+  if (!parts || n_parts < 1) {
+    g_create_error = "nf_split_create: no parts";
+    return nullptr;
+  }
+  auto sp = std::make_unique<nf_split>();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  try {
+    const nf_params& p0 = parts[0] ? parts[0]->p : nf_params{};
+    for (int i = 0; i < n_parts; i++) {
+      nf_solver* s = parts[i];
+      if (!s) throw std::invalid_argument("nf_split_create: null part");
+      if (s->p.precision != p0.precision || s->p.time_scheme != p0.time_scheme ||
+          s->p.spatial_order != p0.spatial_order || s->p.local_time_stepping != p0.local_time_stepping ||
+          s->p.dt_from_current_state != p0.dt_from_current_state)
+        throw std::invalid_argument("nf_split_create: the parts' solver parameters differ");
+      if (s->stage_next != 0) throw std::invalid_argument("nf_split_create: a part is inside a step");
+      for (int j = 0; j < i; j++)
+        if (parts[j] == s) throw std::invalid_argument("nf_split_create: a part is listed twice");
+      sp->parts.push_back(s);
+    }
+    sp->global_dt = !p0.local_time_stepping;
+    for (int i = 0; i < n_parts; i++) {
+      sp->set_dev(parts[i]->device);
+      cudaEvent_t a, b;
+      ck(cudaEventCreateWithFlags(&a, cudaEventDisableTiming), "cudaEventCreate");
+      sp->ready.push_back(a);
+      ck(cudaEventCreateWithFlags(&b, cudaEventDisableTiming), "cudaEventCreate");
+      sp->copied.push_back(b);
+      // peer access between every pair of devices the parts use
+      for (int j = 0; j < n_parts; j++) {
+        const int d = parts[j]->device;
+        if (d == parts[i]->device) continue;
+        int ok = 0;
+        ck(cudaDeviceCanAccessPeer(&ok, parts[i]->device, d), "cudaDeviceCanAccessPeer");
+        if (!ok) throw std::invalid_argument("nf_split_create: devices without peer access");
+        const cudaError_t e = cudaDeviceEnablePeerAccess(d, 0);
+        if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
+        else ck(e, "cudaDeviceEnablePeerAccess");
+      }
+    }
+    sp->set_dev(parts[0]->device);
+    ck(cudaEventCreateWithFlags(&sp->dt_done, cudaEventDisableTiming), "cudaEventCreate");
+    std::vector<double*> sc;
+    for (int i = 0; i < n_parts; i++) sc.push_back(parts[i]->scal.p);
+    sp->scal_ptrs.alloc(sc.size());
+    ck(cudaMemcpy(sp->scal_ptrs.p, sc.data(), sc.size() * sizeof(double*), cudaMemcpyHostToDevice), "H2D");
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    cudaSetDevice(dev);
+    return nullptr;
+  }
+  cudaSetDevice(dev);
+  return sp.release();
+}
+
+int nf_split_link(nf_split* sp, int from, int to, const int64_t* from_cells, const int64_t* to_cells, int64_t n) {
+  return split_guarded(sp, [&]() -> int {
+    const int np = int(sp->parts.size());
+    if (from < 0 || from >= np || to < 0 || to >= np || from == to || n < 0 || (n > 0 && (!from_cells || !to_cells))) {
+      sp->err = "nf_split_link: bad part index, count or null cell list";
+      return NF_ERR_ARG;
+    }
+    const int64_t na = sp->parts[size_t(from)]->n, nb = sp->parts[size_t(to)]->n;
+    for (int64_t i = 0; i < n; i++)
+      if (from_cells[i] < 0 || from_cells[i] >= na || to_cells[i] < 0 || to_cells[i] >= nb) {
+        sp->err = "nf_split_link: cell index out of range at entry " + std::to_string(i);
+        return NF_ERR_ARG;
+      }
+    if (n == 0) return NF_OK;
+    auto lk = std::make_unique<nf_split::Link>();
+    lk->from = from;
+    lk->to = to;
+    lk->n = n;
+    nf_solver* b = sp->parts[size_t(to)];
+    sp->set_dev(b->device);
+    lk->from_cells.alloc(size_t(n));
+    lk->to_cells.alloc(size_t(n));
+    ck(cudaMemcpy(lk->from_cells.p, from_cells, size_t(n) * sizeof(int64_t), cudaMemcpyHostToDevice), "H2D");
+    ck(cudaMemcpy(lk->to_cells.p, to_cells, size_t(n) * sizeof(int64_t), cudaMemcpyHostToDevice), "H2D");
+    sp->links.push_back(std::move(lk));
+    return NF_OK;
+  });
+}
+
+int nf_split_advance(nf_split* sp, int64_t n_steps) {
+  return split_guarded(sp, [&]() -> int {
+    if (n_steps < 0) return NF_ERR_ARG;
+    for (nf_solver* s : sp->parts)
+      if (s->stage_next != 0) {
+        sp->err = "nf_split_advance: a part is inside a step";
+        return NF_ERR_ARG;
+      }
+    for (int64_t k = 0; k < n_steps; k++) sp->step();
+    return NF_OK;
+  });
+}
+
+int nf_split_synchronize(nf_split* sp) {
+  return split_guarded(sp, [&]() -> int {
+    for (nf_solver* s : sp->parts) {
+      sp->set_dev(s->device);
+      const int rc = s->check_status();
+      if (rc != NF_OK) {
+        sp->err = s->err;
+        return rc;
+      }
+    }
+    return NF_OK;
+  });
+}
+
+const char* nf_split_last_error(const nf_split* sp) { return sp ? sp->err.c_str() : g_create_error.c_str(); }
+
+void nf_split_destroy(nf_split* sp) {
+  if (!sp) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  delete sp;
+  cudaSetDevice(dev);
 }
 
 }  // extern "C"

@@ -6,8 +6,12 @@ compact and its surface small. Each part is extended by ``layers`` layers of
 neighbouring cells (its halo). Its local mesh lists the owned cells, then the
 halo cells layer by layer, each group in global order, with the boundary
 markers of those cells; the faces where the halo is cut off are left
-unlisted, which NetFlux drops (FV_Grid.cpp:79-85). They touch only the
-outermost halo layer, whose results are never used.
+unlisted, which NetFlux drops (FV_Grid.cpp:79-85), or listed under a marker
+of their own (``cut_marker``, a far field by default). They touch only the
+outermost halo layer, whose results are never used; as a far field they keep
+those cells' throwaway updates physical (with the ghost at the free stream, a
+uniform flow crosses them undisturbed), so a solver's validity checks stay
+quiet there.
 
 Why two layers per stage: the flux balance of an owned cell reads its
 neighbours' face states, which need the neighbours' gradients and limiters,
@@ -20,11 +24,11 @@ TVD-RK3 step), trading redundant halo work for fewer exchanges.
 one part fill which halo cells of the other. The same lists drive an
 exchange over gloo on the CPU and over NCCL between GPUs.
 """
-from typing import Dict, List
+from typing import Dict, List, Optional
 
 import numpy as np
 
-from .meshgen import TetMesh
+from .meshgen import FAR_FIELD, TetMesh
 
 # the face opposite vertex q of a tetrahedron: the other three vertices
 _FACE_VERTS = np.array([[1, 2, 3], [0, 2, 3], [0, 1, 3], [0, 1, 2]])
@@ -52,11 +56,14 @@ def cell_neighbours(tets: np.ndarray) -> np.ndarray:
     return nb.reshape(n, 4)
 
 
-def partition(mesh: TetMesh, sfc_rank: np.ndarray, n_parts: int, layers: int = 2) -> List[Dict[str, np.ndarray]]:
+def partition(mesh: TetMesh, sfc_rank: np.ndarray, n_parts: int, layers: int = 2,
+              cut_marker: Optional[str] = None, cut_type: str = FAR_FIELD) -> List[Dict[str, np.ndarray]]:
     """Split the cells into ``n_parts`` contiguous ranges of ``sfc_rank`` (each cell's position along
     the curve) and add ``layers`` halo layers to each. Every part holds ``cells`` (global ids, owned
     first, then the halo by layer), ``n_owned``, ``layer`` (0 for owned cells, else the halo layer)
-    and ``mesh`` (its local TetMesh, cells in the order of ``cells``)."""
+    and ``mesh`` (its local TetMesh, cells in the order of ``cells``). With ``cut_marker``, each
+    part mesh lists the faces where its halo is cut off under a marker of that name and boundary
+    type ``cut_type``."""
     n = mesh.n_cells
     if not 1 <= n_parts <= max(n, 1):
         raise ValueError("n_parts must be between 1 and the number of cells")
@@ -83,14 +90,22 @@ def partition(mesh: TetMesh, sfc_rank: np.ndarray, n_parts: int, layers: int = 2
             groups.append(new)
             front = new
         cells = np.concatenate(groups)
+        extra = None
+        if cut_marker is not None:
+            # faces of the part's cells whose neighbour cell is outside the part
+            nbc = nb[cells]
+            ci, q = np.nonzero((nbc >= 0) & (level[np.maximum(nbc, 0)] < 0))
+            tets = np.asarray(mesh.tets, dtype=np.int64)
+            extra = [(cut_marker, tets[cells[ci][:, None], _FACE_VERTS[q]], cut_type)]
         parts.append({"cells": cells, "n_owned": int(owned.size), "layer": level[cells],
-                      "owner": owner[cells], "mesh": sub_mesh(mesh, cells)})
+                      "owner": owner[cells], "mesh": sub_mesh(mesh, cells, extra)})
     return parts
 
 
-def sub_mesh(mesh: TetMesh, cells: np.ndarray) -> TetMesh:
+def sub_mesh(mesh: TetMesh, cells: np.ndarray, extra_markers=None) -> TetMesh:
     """The TetMesh of the given cells (in that order): the nodes they use, renumbered in ascending
-    global order, and each marker's triangles that are faces of these cells."""
+    global order, and each marker's triangles that are faces of these cells; ``extra_markers``
+    ((name, triangles in global node ids, boundary type) triples) are appended."""
     cells = np.asarray(cells, dtype=np.int64)
     tets = np.asarray(mesh.tets, dtype=np.int64)[cells]
     used = np.unique(tets)
@@ -110,8 +125,12 @@ def sub_mesh(mesh: TetMesh, cells: np.ndarray) -> TetMesh:
         pos = _search_rows(fk, tk)
         keep = pos >= 0
         markers.append((name, new_id[tris[keep]]))
+    patch_types = dict(mesh.patch_types)
+    for name, tris, btype in extra_markers or []:
+        markers.append((name, new_id[np.asarray(tris, dtype=np.int64).reshape(-1, 3)]))
+        patch_types[name] = btype
     return TetMesh(nodes=np.asarray(mesh.nodes)[used], tets=new_id[tets], markers=markers,
-                   patch_types=dict(mesh.patch_types))
+                   patch_types=patch_types)
 
 
 def _search_rows(sorted_rows: np.ndarray, rows: np.ndarray) -> np.ndarray:

@@ -2,16 +2,18 @@
 
 The cells are split along the Hilbert curve with two halo layers
 (partition.partition) and every part runs on its own EulerSolver, on one
-device or one device per part. Before every stage the primitives of each
-part's halo cells are replaced by those of the cells' owners: the owner
-gathers them on its device (nf_halo_pack), the buffer is copied to the
-receiving part's device (a peer copy when the devices differ) and scattered
-there (nf_halo_unpack). With two layers and an exchange per stage the owned
-cells step exactly as in the undivided mesh (see partition.py). The time step
-is each part's local dt (local time stepping) or, for a global dt, the
-minimum over the parts, set on every part: a part's minimum covers its owned
-and halo cells, whose primitives are the owners' after the exchange, so the
-minimum over parts is the undivided mesh's.
+device or one device per part. The library steps the parts together
+(nf_split_*): before every stage each halo cell takes its owner's primitives
+and conserved stage input, written by a kernel on the receiving part's stream
+that reads the owner's buffers (on the same GPU, or on a peer GPU over
+NVLink), with the parts' streams ordered by events, so the host waits on
+nothing inside a step.
+The time step is each part's local dt (local time stepping) or, for a global
+dt, the minimum over the parts, reduced on the device into every part: a
+part's minimum covers its owned and halo cells, whose primitives are the
+owners' after the exchange, so the minimum over parts is the undivided mesh's.
+With two layers and an exchange per stage the owned cells step exactly as in
+the undivided mesh (see partition.py).
 
 The reference's MPI decomposition is a commented-out sketch
 (src/parallelization/Decomposition.cpp:3-51, README.md:10 lists it as future
@@ -20,7 +22,7 @@ work); this is the device-side exchange for the Hilbert-range decomposition.
 from __future__ import annotations
 
 import ctypes as C
-from typing import Dict, List, Optional, Sequence
+from typing import List, Optional, Sequence
 
 import numpy as np
 
@@ -30,29 +32,32 @@ from . import solver as S
 from .meshgen import TetMesh
 
 
-def _check(rc: int, handle) -> None:
-    if rc != L.NF_OK:
-        raise L.NetFluxError(rc, L.last_error(handle))
+CUT_MARKER = "halo_cut"
 
 
 class SplitSolver:
     """``n_parts`` EulerSolvers over the Hilbert-range parts of ``mesh`` (devices[k] for part k, all on
-    the current device by default). ``U0`` is the initial state in the mesh's cell order."""
+    the current device by default). ``U0`` is the initial state in the mesh's cell order.
+    ``exchange=False`` leaves the halos unexchanged (each part then steps on its own)."""
 
     def __init__(self, config: S.Config, mesh: TetMesh, U0: np.ndarray, n_parts: int, layers: int = 2,
-                 devices: Optional[Sequence[int]] = None, patch_states=None):
-        import torch
-        self.torch = torch
-        self.config = config
+                 devices: Optional[Sequence[int]] = None, patch_states=None, exchange: bool = True):
         if layers < 2:
             raise ValueError("an exchange per stage needs two halo layers")
+        self.config = config
         whole = S.Mesh.from_tet_mesh(mesh)
         rank = whole.permutation()  # each cell's position along the Hilbert curve
         whole.close()
         self.n_cells = mesh.n_cells
-        self.parts = P.partition(mesh, rank, n_parts, layers)
+        # the cut faces of each part as a far field at the free stream: the outermost halo cells'
+        # updates (overwritten by the exchange) stay physical, so the parts' validity checks report
+        # only real failures
+        self.parts = P.partition(mesh, rank, n_parts, layers, cut_marker=CUT_MARKER)
         self.plan = P.exchange_plan(self.parts)
-        self.devices = list(devices) if devices is not None else [torch.cuda.current_device()] * n_parts
+        if devices is None:
+            import torch
+            devices = [torch.cuda.current_device()] * n_parts
+        self.devices = list(devices)
         if len(self.devices) != n_parts:
             raise ValueError("one device per part")
         U0 = np.ascontiguousarray(U0, np.float64)
@@ -61,65 +66,43 @@ class SplitSolver:
         for k, part in enumerate(self.parts):
             m = S.Mesh.from_tet_mesh(part["mesh"])
             self.meshes.append(m)
-            states = None if patch_states is None else [patch_states[pp["name"]] for pp in m.patches()]
+            states = None if patch_states is None else [patch_states.get(pp["name"]) for pp in m.patches()]
             self.solvers.append(S.EulerSolver(config, m, U0=U0[part["cells"]], patch_states=states,
                                               device=self.devices[k]))
-        # per (sender, receiver): device cell lists on both sides and a buffer on each device
-        self.links = []
-        for p, dests in self.plan.items():
-            dev_p = self.meshes[p].permutation()
-            for q, lists in dests.items():
-                dev_q = self.meshes[q].permutation()
-                n = int(lists["send"].size)
-                dp, dq = f"cuda:{self.devices[p]}", f"cuda:{self.devices[q]}"
-                self.links.append({
-                    "p": p, "q": q, "n": n,
-                    "send": torch.tensor(dev_p[lists["send"]], dtype=torch.int64, device=dp),
-                    "recv": torch.tensor(dev_q[lists["recv"]], dtype=torch.int64, device=dq),
-                    "buf_p": torch.empty((5, n), dtype=torch.float64, device=dp),
-                    "buf_q": torch.empty((5, n), dtype=torch.float64, device=dq)})
-        self.n_stages = 3 if config.get_time_scheme() == L.NF_TVD_RK3 else 1
-
-    def exchange(self) -> None:
-        """Every halo cell takes its owner's primitives (those the next stage reads)."""
         lib = L.load()
-        for ln in self.links:
-            sp, sq = self.solvers[ln["p"]], self.solvers[ln["q"]]
-            _check(lib.nf_halo_pack(sp._h, C.c_void_p(ln["send"].data_ptr()), ln["n"],
-                                    C.c_void_p(ln["buf_p"].data_ptr())), sp._h)
-            ln["buf_q"].copy_(ln["buf_p"])  # device to device (peer copy across devices)
-            self.torch.cuda.synchronize(ln["buf_q"].device)
-            _check(lib.nf_halo_unpack(sq._h, C.c_void_p(ln["recv"].data_ptr()), ln["n"],
-                                      C.c_void_p(ln["buf_q"].data_ptr())), sq._h)
+        handles = (C.c_void_p * n_parts)(*[s._h for s in self.solvers])
+        self._h = lib.nf_split_create(handles, n_parts)
+        if not self._h:
+            raise L.NetFluxError(L.NF_ERR_ARG, lib.nf_split_last_error(None).decode())
+        self.n_halo_values = 0
+        if exchange:
+            # the plan in each part's device numbering
+            perm = [m.permutation() for m in self.meshes]
+            for p, dests in self.plan.items():
+                for q, lists in dests.items():
+                    a = np.ascontiguousarray(perm[p][lists["send"]], np.int64)
+                    b = np.ascontiguousarray(perm[q][lists["recv"]], np.int64)
+                    self._check(lib.nf_split_link(self._h, p, q, L.i64ptr(a), L.i64ptr(b), a.size))
+                    self.n_halo_values += 5 * a.size
 
-    def calc_timestep(self) -> float:
-        """Each part's time step; with a global dt their minimum, set on every part."""
-        dts = []
-        for s in self.solvers:
-            s.calc_timestep(self.config)
-            dts.append(self.config.get_delta_time())
-        dt = min(dts)
-        if not self.config.local_time_stepping:
-            for s in self.solvers:
-                s.set_timestep(dt)
-        self.config.set_delta_time(dt)
-        return dt
+    def _check(self, rc: int) -> None:
+        if rc != L.NF_OK:
+            raise L.NetFluxError(rc, L.load().nf_split_last_error(self._h).decode())
 
     def step(self) -> None:
-        """calc_timestep, then every stage after a halo exchange."""
-        lib = L.load()
-        self.calc_timestep()
-        for stage in range(self.n_stages):
-            self.exchange()
-            for s in self.solvers:
-                _check(lib.nf_stage(s._h, stage), s._h)
+        """calc_timestep, then every stage after a halo exchange (queued on the devices)."""
+        self.advance(1)
 
     def advance(self, n_steps: int) -> None:
-        for _ in range(n_steps):
-            self.step()
+        self._check(L.load().nf_split_advance(self._h, n_steps))
+
+    def synchronize(self) -> None:
+        """Wait for every part; raises on the first part whose status reports a failure."""
+        self._check(L.load().nf_split_synchronize(self._h))
 
     def get_solution(self) -> np.ndarray:
         """The owned cells' states, in the mesh's cell order."""
+        self.synchronize()
         U = np.empty((self.n_cells, 5))
         for part, s in zip(self.parts, self.solvers):
             Up = s.get_solver_data().get_solution()
@@ -128,8 +111,11 @@ class SplitSolver:
         return U
 
     def close(self) -> None:
+        if getattr(self, "_h", None):
+            L.load().nf_split_destroy(self._h)
+            self._h = None
         for s in self.solvers:
             s.close()
         for m in self.meshes:
             m.close()
-        self.solvers, self.meshes, self.links = [], [], []
+        self.solvers, self.meshes = [], []

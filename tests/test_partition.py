@@ -84,14 +84,16 @@ def test_parts_with_exchange_match_the_undivided_mesh(time_scheme, layers, steps
 
 
 @pytest.mark.parametrize("global_dt", [False, True])
-def test_rk3_with_two_layers_and_an_exchange_per_stage(global_dt):
+@pytest.mark.parametrize("cut_marker", [None, "halo_cut"])
+def test_rk3_with_two_layers_and_an_exchange_per_stage(global_dt, cut_marker):
     """The production plan: 2 halo layers, the halo states exchanged after every TVD-RK3 stage, and
-    with a global time step the minimum taken over the owned cells of all parts (an all-reduce)."""
+    with a global time step the minimum taken over the owned cells of all parts (an all-reduce).
+    The cut faces dropped or listed as a far field: the owned cells step the same either way."""
     m, fs, mm, U0 = _case()
     pats = mm.patches()
     ref = po.run_oracle(mm.export(), pats, [fs] * len(pats), U0, 3, time_scheme=1,
                         local_time_stepping=not global_dt, dt_from_current_state=True, fields=False)["U"]
-    parts = P.partition(m, mm.permutation(), 3, layers=2)
+    parts = P.partition(m, mm.permutation(), 3, layers=2, cut_marker=cut_marker)
     plan = P.exchange_plan(parts)
     so = []
     for p in parts:
@@ -111,6 +113,28 @@ def test_rk3_with_two_layers_and_an_exchange_per_stage(global_dt):
     for p, u in zip(parts, U):
         out[p["cells"][:p["n_owned"]]] = u[:p["n_owned"]]
     assert _rel_linf(out, ref) <= 1e-12
+
+
+def test_cut_marker_lists_exactly_the_cut_faces():
+    """With cut_marker every face between a part's cells and the rest of the mesh is listed under
+    that marker (a far field by default), once, and every such face belongs to an outermost-layer
+    cell."""
+    m = mg.bump_mesh(8, 4, 4, h=0.1)
+    nb = P.cell_neighbours(m.tets)
+    for layers in (1, 2):
+        for p in P.partition(m, np.arange(m.n_cells), 3, layers=layers, cut_marker="cut",
+                             cut_type=mg.SLIP_WALL if layers == 1 else mg.FAR_FIELD):
+            pm = p["mesh"]
+            assert pm.patch_types["cut"] == (mg.SLIP_WALL if layers == 1 else mg.FAR_FIELD)
+            inside = np.zeros(m.n_cells, bool)
+            inside[p["cells"]] = True
+            nbc = nb[p["cells"]]
+            ci, q = np.nonzero((nbc >= 0) & ~inside[np.maximum(nbc, 0)])
+            assert np.all(p["layer"][ci] == layers)
+            cut = np.sort(dict(pm.markers)["cut"], axis=1)
+            local = np.sort(np.asarray(pm.tets)[ci[:, None], P._FACE_VERTS[q]], axis=1)
+            assert cut.shape == local.shape
+            assert np.array_equal(cut[np.lexsort(cut.T[::-1])], local[np.lexsort(local.T[::-1])])
 
 
 def test_too_few_layers_is_not_exact():
