@@ -482,9 +482,6 @@ __device__ __forceinline__ void stage_t(uint8_t* dst, const __nv_bfloat16* src, 
       *reinterpret_cast<uint4*>(dst + umma::kmaj_off(ch * 8 + q, rg * 8, KC)) = column8(v, q);
   }
 }
-__device__ __forceinline__ void stage_t128(uint8_t* dst, const __nv_bfloat16* src, int64_t b0, int64_t B) {
-  stage_t<H>(dst, src, b0, B);
-}
 __device__ __forceinline__ void stage_t16(uint8_t* dst, const __nv_bfloat16* src, int64_t b0, int64_t B) {
   stage_t<16>(dst, src, b0, B);
 }
@@ -494,19 +491,43 @@ struct WgBuf {
   uint8_t* B[3];  // [H0|1]^T, [H1|1]^T, [H2|1]^T
   uint8_t* X;     // X0^T
   uint8_t* D4;    // dZ4^T
-  __device__ explicit WgBuf(uint8_t* base) {
+  uint8_t* base;
+  __device__ explicit WgBuf(uint8_t* base_) : base(base_) {
     for (int i = 0; i < 5; i++) A[i] = base + i * WG_A;
     for (int i = 0; i < 3; i++) B[i] = base + 5 * WG_A + i * WG_BA;
     X = base + 5 * WG_A + 3 * WG_BA;
     D4 = X + WG_B16;
   }
-  // the chunk of KC batch rows from b0, transposed into K-major operands
+  // the chunk of KC batch rows from b0, transposed into K-major operands. The
+  // tasks of the eight 128-feature operands (one 8-feature chunk of 8 rows
+  // each) are spread over all threads, two per thread with both tasks' loads
+  // issued before either's stores, so no thread runs the operands one after
+  // another while the others wait at the barrier.
   __device__ void stage(const WgArgs& a, int64_t b0) {
+    constexpr int kPer = (H / 8) * (KC / 8), kWide = 8 * kPer;
+    static_assert(kWide == 2 * WG_THREADS, "two wide tasks per thread");
+    uint4 v[2][8];
+    int ch[2], rg[2];
+    uint8_t* dst[2];
 #pragma unroll
-    for (int l = 0; l < 4; l++) stage_t128(A[l], a.dz + int64_t(l) * a.B * H, b0, a.B);
-    stage_t128(A[4], a.save + save_h(a.B, 3), b0, a.B);
+    for (int u = 0; u < 2; u++) {
+      const int task = threadIdx.x + u * WG_THREADS, op = task / kPer, lt = task % kPer;
+      ch[u] = lt % (H / 8);
+      rg[u] = lt / (H / 8);
+      // operands 0-3: dZ0..dZ3; 4: H3; 5-7: H0..H2
+      const __nv_bfloat16* src = op < 4 ? a.dz + int64_t(op) * a.B * H : a.save + save_h(a.B, op == 4 ? 3 : op - 5);
+      dst[u] = op < 5 ? base + op * WG_A : base + 5 * WG_A + (op - 5) * WG_BA;  // A[op] or B[op - 5]
 #pragma unroll
-    for (int l = 0; l < 3; l++) stage_t128(B[l], a.save + save_h(a.B, l), b0, a.B);
+      for (int r = 0; r < 8; r++) {
+        const int64_t b = b0 + rg[u] * 8 + r;
+        v[u][r] = b < a.B ? *reinterpret_cast<const uint4*>(src + b * H + ch[u] * 8) : make_uint4(0u, 0u, 0u, 0u);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 2; u++)
+#pragma unroll
+      for (int q = 0; q < 8; q++)
+        *reinterpret_cast<uint4*>(dst[u] + umma::kmaj_off(ch[u] * 8 + q, rg[u] * 8, KC)) = column8(v[u], q);
     stage_t16(X, a.save + save_x0(a.B), b0, a.B);
     stage_t16(D4, a.dz4, b0, a.B);
   }
