@@ -170,9 +170,9 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
     FP64 (gradient_node / flux_node), per cell:
       gradient: V (40), 4 vertex ids (16), 4 neighbour ids (16), face code (4),
         vol (8), writes 4 face states (160); per node 32 (xyz + pad); per
-        boundary face one ghost state (40); the last stage also reads dS (24)
-        and writes the next step's dt (8 with local time stepping): a third of
-        that on average.
+        boundary face one ghost state (40); the last stage also writes the
+        next step's dt (8 with local time stepping; its projected areas come
+        from the normals in registers): a third of that on average.
       flux: 4 own face states (160), 4 neighbour face ids (16), face code (4),
         4 vertex ids (16), U (40), U^n (40 at stages 2 and 3: 2/3 on average),
         vol (8), local dt (8 with local time stepping), writes U and V (80) and
@@ -191,7 +191,7 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
         grad = n_cells * (40 + 16 + 16 + 4 + 8 + 80) + n_nodes * 16 + n_boundary * 40
         flux = n_cells * (40 + 80 + 16 + 4 + 16 + upd) + n_nodes * 16 + n_boundary * 20
     else:
-        grad = n_cells * (40 + 16 + 16 + 4 + 8 + 160 + (24 + lts) / 3) + n_nodes * 32 + n_boundary * 40
+        grad = n_cells * (40 + 16 + 16 + 4 + 8 + 160 + lts / 3) + n_nodes * 32 + n_boundary * 40
         flux = n_cells * (160 + 16 + 4 + 16 + upd) + n_nodes * 32 + n_boundary * 40
     return {"flux": flux, "gradient": grad}
 

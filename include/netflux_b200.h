@@ -278,7 +278,9 @@ int nf_halo_unpack(nf_solver* s, const int64_t* cells, int64_t n, const double* 
  * own GPU, or a peer GPU over NVLink), the parts' streams ordered by events,
  * then the stage on every part. nf_split_synchronize waits for the parts and returns the first
  * failing part's status. A part must not be stepped on its own while it is in
- * a split. NULL from nf_split_create: nf_split_last_error(NULL). No
+ * a split, and the split is destroyed before its parts (nf_split_destroy
+ * waits for their streams). NULL from nf_split_create:
+ * nf_split_last_error(NULL). No
  * counterpart in the reference (Decomposition.cpp:3-51 is a commented-out
  * sketch). */
 typedef struct nf_split nf_split;

@@ -575,8 +575,9 @@ __device__ __forceinline__ void face_normals(const T P[4][3], T S[4][3]) {
 // at the cost of registers); 3 as 0, with the cell's own rows prefetched
 // into L2 first.
 // The body for one cell; vown receives the cell's own primitives.
-template <typename T, int kPipe>
-__device__ __forceinline__ void gradient_node_cell(const MeshView<T>& m, const StageArgs& a, int c, T vown[5]) {
+template <typename T, int kPipe, bool kDS = false>
+__device__ __forceinline__ void gradient_node_cell(const MeshView<T>& m, const StageArgs& a, int c, T vown[5],
+                                                   T* dS_out = nullptr) {
   const int st = m.stride;
   static_assert(sizeof(T) == 8, "FP64 kernel");
   const T* __restrict__ Vin = a.Vin;
@@ -635,6 +636,17 @@ __device__ __forceinline__ void gradient_node_cell(const MeshView<T>& m, const S
   }
   const T ssum[3] = {(S[0][0] + S[1][0]) + (S[2][0] + S[3][0]), (S[0][1] + S[1][1]) + (S[2][1] + S[3][1]),
                      (S[0][2] + S[1][2]) + (S[2][2] + S[3][2])};
+  if constexpr (kDS) {
+    // projected areas of calc_Delta_S (Solver.cpp:276-298): half the sum of
+    // |S_d| over the cell's interior faces, from the normals in registers
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+      T acc = T(0);
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc += nb[q] >= 0 ? fabs(S[q][e]) : T(0);
+      dS_out[e] = T(0.5) * acc;
+    }
+  }
   const T hv = T(0.5) * nr_rcp(T(m.vol[c]));
   const bool rat = a.barth && ratchet_on(a, c);
   auto variable = [&](int k, T vc, const T vo[4]) {
@@ -717,20 +729,15 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
   pdl_wait_previous();
   const bool in = c < m.n;
   const bool active = in && !frozen_cell(a, c);
-  if (kDt && active) {  // the time step's own rows: into L2 now, read after the gradient work
-#pragma unroll
-    for (int e = 0; e < 3; e++) prefetch_l2(m.dS + size_t(e) * m.stride + c);
-  }
-  T vown[5];
-  if (active) gradient_node_cell<T, kPipe>(m, a, c, vown);
+  T vown[5], dS[3];
+  if (active) gradient_node_cell<T, kPipe, kDt>(m, a, c, vown, dS);
   if constexpr (kDt) {
     double dtc = DBL_MAX;
     if (in) {
-      const int st = m.stride;
       if (!active) {
         if (dtf.dt_next) dtf.dt_next[c] = 0.0;  // a converged case keeps its state
       } else {
-        const double d = dt_of_cell_fast(vown, m.dS[c], m.dS[st + c], m.dS[2 * st + c], m.vol[c], dtf.cfl);
+        const double d = dt_of_cell_fast(vown, dS[0], dS[1], dS[2], m.vol[c], dtf.cfl);
         if (dtf.dt_next) dtf.dt_next[c] = d;
         if (!(d > 0.0) && !isnan(d)) atomicOr(a.status, kErrDt);
         if (d > 0.0) dtc = d;  // std::min skips NaN (comparisons with NaN are false)

@@ -175,6 +175,19 @@ def _oracle(g, n, **kw):
     return po.run_oracle(m.export(), pats, [g["freestream"]] * len(pats), g["U0"], n, **kw)
 
 
+def test_fused_time_step_matches_oracle():
+    """FP64: from the second step on, the time step comes from the last stage's gradient kernel
+    (the last stage input's primitives, projected areas from the normals in registers, the fast
+    reciprocals); each step's dt agrees with the oracle's calc_timestep to a few ulp."""
+    g = golden("bump12")
+    _, U, dts = run(g, "fp64", 20)
+    o = _oracle(g, 20, fields=False)
+    err = np.abs(dts - o["dt"]) / o["dt"]
+    print("fused dt vs oracle: max rel", err.max())
+    assert err.max() <= 1e-14
+    assert rel_linf(U, o["U"]) <= 1e-12
+
+
 def test_local_time_stepping_matches_oracle():
     g = golden("bump12")
     _, U, _ = run(g, "fp64_ref", 10, local_time_stepping=True)
