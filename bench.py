@@ -199,11 +199,11 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
 # DRAM bytes per cell of one launch (dram__bytes_read.sum + dram__bytes_write.sum), captured
 # with ncu on the full 3,145,728-tet bump channel with the tuned launch shapes, averaged over the
 # three stages of a step like the event-timed launch durations (FP64: gradient 64/7, flux 64/9,
-# stages 753.5 / 752.7 / 856.1 and 1100.4 / 1211.2 / 1215.1 MB; mixed: gradient 64/7, flux
+# stages 755.3 / 749.8 / 780.6 and 1108.6 / 1221.7 / 1227.9 MB; mixed: gradient 64/7, flux
 # 128/8, stages 503.3 / 501.1 / 500.4 and 978.2 / 1095.4 / 1090.5 MB); the bump workload's
 # `roofline.traffic` is this times its cells, other workloads report null.
 MEASURED_DRAM_BYTES_PER_CELL = {
-    ("fp64", "gradient"): 787.4e6 / 3145728, ("fp64", "flux"): 1175.6e6 / 3145728,
+    ("fp64", "gradient"): 761.9e6 / 3145728, ("fp64", "flux"): 1186.1e6 / 3145728,
     ("mixed", "gradient"): 501.6e6 / 3145728, ("mixed", "flux"): 1054.7e6 / 3145728,
 }
 

@@ -225,9 +225,10 @@ int nf_snapshot_wait(nf_solver* s);
  * that state the solver's state exactly as nf_set_state does, queued on the
  * device after the work already queued and after the copy, and returns
  * without waiting; NF_ERR_ARG without a begin. The next begin may follow at
- * once (its copy waits on the device until the committed state has been
- * taken from the staging buffer). nf_upload_wait blocks until the last
- * upload's copy has landed, after which its host buffer may change.
+ * once: uploads use two device staging buffers in turn, so its copy waits on
+ * the device only for the state committed two uploads back to have been
+ * taken. nf_upload_wait blocks until every upload's copy has landed, after
+ * which their host buffers may change.
  * Together with the snapshots this streams independent states through one
  * solver with both copies overlapping the steps and the host never waiting
  * on a copy. No counterpart in the reference (it has no device memory). */

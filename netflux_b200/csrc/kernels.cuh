@@ -460,25 +460,16 @@ __device__ __forceinline__ double dt_of_cell(const double V[5], double dS0, doub
   return __ddiv_rn(__dmul_rn(cfl, vol), __dadd_rn(__dadd_rn(sx, sy), sz));
 }
 
-// Minimum of v over the block, then one atomicMin on the bit pattern (exact
-// and order-free for positive doubles). Every thread of the block calls it.
-__device__ __forceinline__ void block_min_to(double v, unsigned long long* target) {
+// Minimum of v over the warp, then one atomicMin on the bit pattern (exact
+// and order-free for positive doubles), skipped when the warp's minimum is not
+// below the current one (the value only decreases, so the result is the same
+// exact minimum); no block barrier. Every lane of the warp calls it.
+__device__ __forceinline__ void warp_min_to(double v, unsigned long long* target) {
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, off));
-  __shared__ double wmin[32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) wmin[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    v = (lane < int(blockDim.x + 31) / 32) ? wmin[lane] : DBL_MAX;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, off));
-    // a block whose minimum is not below the current one skips the atomic
-    // (the value only decreases, so the result is the same exact minimum)
-    if (lane == 0 && v < DBL_MAX &&
-        v < __longlong_as_double(static_cast<long long>(*reinterpret_cast<volatile unsigned long long*>(target))))
-      atomicMin(target, (unsigned long long)__double_as_longlong(v));
-  }
+  if ((threadIdx.x & 31) == 0 && v < DBL_MAX &&
+      v < __longlong_as_double(static_cast<long long>(*reinterpret_cast<volatile unsigned long long*>(target))))
+    atomicMin(target, (unsigned long long)__double_as_longlong(v));
 }
 
 // The next step's time step, computed by the FP64 form's last-stage gradient
@@ -575,6 +566,16 @@ __device__ __forceinline__ void face_normals(const T P[4][3], T S[4][3]) {
 // at the cost of registers); 3 as 0, with the cell's own rows prefetched
 // into L2 first.
 // The body for one cell; vown receives the cell's own primitives.
+// CFL time step of one cell from its primitives with the fast forms'
+// reciprocal and reciprocal square root (within 2 ulp of dt_of_cell).
+__device__ __forceinline__ double dt_of_cell_fast(const double V[5], double dS0, double dS1, double dS2, double vol,
+                                                  double cfl) {
+  const double g = Gas<double>::gamma * V[4];
+  const double cs = g * nr_rsqrt(g * V[0]);  // sqrt(gamma p / rho)
+  const double sum = fma(fabs(V[3]) + cs, dS2, fma(fabs(V[2]) + cs, dS1, (fabs(V[1]) + cs) * dS0));
+  return cfl * vol * nr_rcp(sum);
+}
+
 template <typename T, int kPipe, bool kDS = false>
 __device__ __forceinline__ void gradient_node_cell(const MeshView<T>& m, const StageArgs& a, int c, T vown[5],
                                                    T* dS_out = nullptr) {
@@ -707,15 +708,6 @@ __device__ __forceinline__ void gradient_node_cell(const MeshView<T>& m, const S
   }
 }
 
-// CFL time step of one cell from its primitives with the fast forms'
-// reciprocal and reciprocal square root (within 2 ulp of dt_of_cell).
-__device__ __forceinline__ double dt_of_cell_fast(const double V[5], double dS0, double dS1, double dS2, double vol,
-                                                  double cfl) {
-  const double g = Gas<double>::gamma * V[4];
-  const double cs = g * nr_rsqrt(g * V[0]);  // sqrt(gamma p / rho)
-  const double sum = fma(fabs(V[3]) + cs, dS2, fma(fabs(V[2]) + cs, dS1, (fabs(V[1]) + cs) * dS0));
-  return cfl * vol * nr_rcp(sum);
-}
 
 // kDt: also the next step's time step from the cell's own primitives, after
 // the gradient work (the FP64 form's last stage; the primitives are those of
@@ -743,7 +735,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView
         if (d > 0.0) dtc = d;  // std::min skips NaN (comparisons with NaN are false)
       }
     }
-    block_min_to(dtc, dtf.dt_min_bits);
+    warp_min_to(dtc, dtf.dt_min_bits);
   }
 }
 

@@ -323,13 +323,19 @@ struct nf_solver {
   bool snap_used[2] = {false, false};
   int snap_k = 0;
   bool snap_pending = false;
-  // asynchronous state uploads (nf_upload_begin / nf_upload_commit): a third
-  // AoS staging buffer, filled from the host on its own stream
-  DevBuf<double> up;
+  // asynchronous state uploads (nf_upload_begin / nf_upload_commit): two
+  // more AoS staging buffers, used in turn and filled from the host on their
+  // own stream, so the next state's copy never waits for the scatter of the
+  // one before it (only for the scatter two uploads back)
+  DevBuf<double> up[2];
   cudaStream_t up_stream = nullptr;
-  cudaEvent_t up_done = nullptr, up_free = nullptr;  // copy landed; scatter done reading `up`
-  bool up_pending = false, up_used = false;
-  bool up_reading = false;  // the last upload's copy may still read the caller's buffer
+  cudaEvent_t up_done[2] = {nullptr, nullptr};  // copy into up[k] landed
+  cudaEvent_t up_free[2] = {nullptr, nullptr};  // the scatter of up[k] is done reading it
+  bool up_used[2] = {false, false};
+  int up_k = 0;    // staging buffer of the next upload
+  int up_cur = 0;  // staging buffer of the upload in flight
+  bool up_pending = false;
+  bool up_reading = false;  // copies may still read the caller's buffers (until nf_upload_wait)
   DevBuf<long long> d_dev_of_ref;  // [N]
 
   // per-kernel timing: events around every launch while prof_on
@@ -729,9 +735,11 @@ struct nf_solver {
     for (auto e : snap_done)
       if (e) cudaEventDestroy(e);
     if (snap_stream) cudaStreamDestroy(snap_stream);
-    if (up_pending || up_reading) cudaEventSynchronize(up_done);  // the copy still reads the caller's memory
-    if (up_done) cudaEventDestroy(up_done);
-    if (up_free) cudaEventDestroy(up_free);
+    if (up_stream) cudaStreamSynchronize(up_stream);  // copies may still read the caller's memory
+    for (int k = 0; k < 2; k++) {
+      if (up_done[k]) cudaEventDestroy(up_done[k]);
+      if (up_free[k]) cudaEventDestroy(up_free[k]);
+    }
     if (up_stream) cudaStreamDestroy(up_stream);
     for (auto& g : graph)
       if (g) cudaGraphExecDestroy(g);
@@ -1486,15 +1494,20 @@ int nf_upload_begin(nf_solver* s, const double* U, int64_t n_cells) {
     }
     if (!s->up_stream) {
       ck(cudaStreamCreateWithFlags(&s->up_stream, cudaStreamNonBlocking), "cudaStreamCreate");
-      ck(cudaEventCreateWithFlags(&s->up_done, cudaEventDisableTiming), "cudaEventCreate");
-      ck(cudaEventCreateWithFlags(&s->up_free, cudaEventDisableTiming), "cudaEventCreate");
+      for (int k = 0; k < 2; k++) {
+        ck(cudaEventCreateWithFlags(&s->up_done[k], cudaEventDisableTiming), "cudaEventCreate");
+        ck(cudaEventCreateWithFlags(&s->up_free[k], cudaEventDisableTiming), "cudaEventCreate");
+      }
     }
-    if (s->up.n != size_t(5) * s->n) s->up.alloc(size_t(5) * s->n);
-    // the previous commit's scatter may still be reading the staging buffer
-    if (s->up_used) ck(cudaStreamWaitEvent(s->up_stream, s->up_free, 0), "cudaStreamWaitEvent");
-    ck(cudaMemcpyAsync(s->up.p, U, size_t(5) * s->n * sizeof(double), cudaMemcpyHostToDevice, s->up_stream),
+    const int k = s->up_k;
+    if (s->up[k].n != size_t(5) * s->n) s->up[k].alloc(size_t(5) * s->n);
+    // the scatter of this staging buffer's previous state may still be reading it
+    if (s->up_used[k]) ck(cudaStreamWaitEvent(s->up_stream, s->up_free[k], 0), "cudaStreamWaitEvent");
+    ck(cudaMemcpyAsync(s->up[k].p, U, size_t(5) * s->n * sizeof(double), cudaMemcpyHostToDevice, s->up_stream),
        "upload H2D");
-    ck(cudaEventRecord(s->up_done, s->up_stream), "cudaEventRecord");
+    ck(cudaEventRecord(s->up_done[k], s->up_stream), "cudaEventRecord");
+    s->up_cur = k;
+    s->up_k = 1 - k;
     s->up_pending = true;
     return NF_OK;
   });
@@ -1508,11 +1521,12 @@ int nf_upload_commit(nf_solver* s) {
     }
     // the solver stream takes the state once the copy has landed; work
     // queued before this call runs first and is not affected
-    ck(cudaStreamWaitEvent(s->stream, s->up_done, 0), "cudaStreamWaitEvent");
-    s->adopt_state(s->up.p);
+    const int k = s->up_cur;
+    ck(cudaStreamWaitEvent(s->stream, s->up_done[k], 0), "cudaStreamWaitEvent");
+    s->adopt_state(s->up[k].p);
     ck(cudaGetLastError(), "nf_upload_commit");
-    ck(cudaEventRecord(s->up_free, s->stream), "cudaEventRecord");
-    s->up_used = true;
+    ck(cudaEventRecord(s->up_free[k], s->stream), "cudaEventRecord");
+    s->up_used[k] = true;
     s->up_pending = false;
     s->up_reading = true;  // until nf_upload_wait: the copy may still read the caller's buffer
     return NF_OK;
@@ -1521,7 +1535,7 @@ int nf_upload_commit(nf_solver* s) {
 
 int nf_upload_wait(nf_solver* s) {
   return guarded(s, [&]() -> int {
-    if (s->up_pending || s->up_reading) ck(cudaEventSynchronize(s->up_done), "upload wait");
+    if ((s->up_pending || s->up_reading) && s->up_stream) ck(cudaStreamSynchronize(s->up_stream), "upload wait");
     s->up_reading = false;
     return NF_OK;
   });
