@@ -9,7 +9,7 @@ The smaller cube and Sod cases fit the L2 and are reported as L2-warm
 figures (config.l2 says which).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--case bump|cube|sod] [--precision fp64|mixed|fp64_ref]
+                    [--case bump|cube|sod] [--precision fp64|mixed|mixed32|fp64_ref]
 
 Prints one JSON line on rank 0. ``value`` is Mcell-RK-stages/s with the state
 resident in HBM (CUDA events on the solver's stream, max over ranks);
@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--case", default="bump", choices=["bump", "cube", "sod"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "fp64_ref"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "mixed32", "fp64_ref"])
     ap.add_argument("--scale", type=int, default=1, help="divide the hex counts (quick runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -184,12 +184,23 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
       flux: own V (40), own increments (80), neighbour face ids (16), code (4),
         vertex ids (16), U, U^n, vol, dt, writes U, V and R_rho as above; per
         node 16; per boundary face an FP32 flux difference (20).
+    Mixed with FP32 copies (the FP32 node kernels, NF_PREC_MIXED32):
+      gradient: FP32 V (20), ids (32), code (4), vol (8), writes 4 FP32 face
+        states (80); per node 16; per boundary face an FP32 ghost (20).
+      flux: 4 own FP32 face states (80), neighbour face ids (16), code (4),
+        vertex ids (16), U, U^n, vol, dt, writes U (40), the FP32 V (20), the
+        FP64 V of the state the next time step reads (40 once a step: 1/3 on
+        average) and R_rho; per node 16; per boundary face an FP32 flux (20).
     """
     lts = 8 if local_dt else 0
     upd = 40 + 40 * 2 / 3 + 8 + lts + 80 + 8 / 3  # U, U^n, vol, dt, U and V out, R_rho
     if precision == "mixed":
         grad = n_cells * (40 + 16 + 16 + 4 + 8 + 80) + n_nodes * 16 + n_boundary * 40
         flux = n_cells * (40 + 80 + 16 + 4 + 16 + upd) + n_nodes * 16 + n_boundary * 20
+    elif precision == "mixed32":
+        upd32 = 40 + 40 * 2 / 3 + 8 + lts + 40 + 20 + 40 / 3 + 8 / 3
+        grad = n_cells * (20 + 16 + 16 + 4 + 8 + 80) + n_nodes * 16 + n_boundary * 20
+        flux = n_cells * (80 + 16 + 4 + 16 + upd32) + n_nodes * 16 + n_boundary * 20
     else:
         grad = n_cells * (40 + 16 + 16 + 4 + 8 + 160 + lts / 3) + n_nodes * 32 + n_boundary * 40
         flux = n_cells * (160 + 16 + 4 + 16 + upd) + n_nodes * 32 + n_boundary * 40
@@ -567,7 +578,7 @@ def main():
             "metric": METRIC, "value": round(value, 3), "unit": "Mcell-stages/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 5),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": {"fp64": "f64", "fp64_ref": "f64", "mixed": "f32+f64"}[args.precision],
+            "dtype": {"fp64": "f64", "fp64_ref": "f64", "mixed": "f32+f64", "mixed32": "f32+f64"}[args.precision],
             "data": "synthetic",
             "config": {"workload": desc, "cells": N, "faces": mesh.n_faces, "time_scheme": "TVD_RK3",
                        "local_time_stepping": lts, "cfl": 0.8, "precision": args.precision,

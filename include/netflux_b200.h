@@ -71,7 +71,14 @@ extern "C" {
                                  reference to the last bit except pow() */
 #define NF_PREC_FP64 1        /* FP64 throughout, FMA and reciprocals allowed */
 #define NF_PREC_MIXED 2       /* FP64 state / RK combine / dt / norms; FP32
-                                 gradient, limiter, reconstruction and flux */
+                                 gradient, limiter, reconstruction and flux in
+                                 differences to the cell's FP64 primitives
+                                 (converges to steady residuals like FP64) */
+#define NF_PREC_MIXED32 3     /* FP64 state / RK combine / dt / norms; FP32
+                                 copies of the primitives, FP32 gradient,
+                                 limiter, reconstruction and flux (faster;
+                                 its steady residual stops near a 1e-5 drop).
+                                 Not for split meshes (nf_split_*, halos) */
 
 /* nf_get_field selectors */
 #define NF_FIELD_SOLUTION 0   /* U  [N][5] */

@@ -24,7 +24,7 @@ NF_EXPLICIT_EULER, NF_TVD_RK3 = 0, 1
 NF_FIRST_ORDER, NF_SECOND_ORDER = 0, 1
 NF_LIMITER_NONE, NF_LIMITER_BARTH = 0, 1
 NF_FLUX_RUSANOV = 0
-NF_PREC_FP64_REF, NF_PREC_FP64, NF_PREC_MIXED = 0, 1, 2
+NF_PREC_FP64_REF, NF_PREC_FP64, NF_PREC_MIXED, NF_PREC_MIXED32 = 0, 1, 2, 3
 (NF_FIELD_SOLUTION, NF_FIELD_PRIMVARS, NF_FIELD_GRADIENT, NF_FIELD_LIMITER,
  NF_FIELD_FLUX_BALANCE, NF_FIELD_LOCAL_DT) = range(6)
 

@@ -123,6 +123,22 @@ struct StageArgs {
   double* vg;
   double* fb;
   float* fb32;
+  // mixed form with FP32 copies (NF_PREC_MIXED32): the FP32 primitives of
+  // the stage input and of its result, and FP32 ghost states [5][bstride];
+  // the face states go to fs32 and the boundary fluxes to fb32. Vout (FP64)
+  // is written only where a later time step reads it (null otherwise).
+  const float* Vin32;
+  float* Vout32;
+  float* vg32;
+  // mixed forms, TVD-RK3: the stage whose result is the last stage's input
+  // (stage 2 of 3) also computes the next step's time step from the FP64
+  // primitives of that result, the ones the reference's calc_timestep reads
+  // (Solver.cpp:250): per cell into dt_next (local time stepping, else null)
+  // and the minimum into *dt_next_min (null: not this stage)
+  double* dt_next;
+  unsigned long long* dt_next_min;
+  const double* dS;  // [3][stride] projected areas (calc_Delta_S)
+  double cfl;
   // converged cases of a steady solve (null: none); their cells are skipped
   // by the fast kernels (cases share no faces, and U is left untouched)
   const int* case_frozen;
@@ -161,6 +177,30 @@ __device__ __forceinline__ T ratchet(const StageArgs& a, size_t at, T phi) {
   keep[at] = v;
   return v;
 }
+
+// The arrays the node kernels read and write, by arithmetic type: FP64 for
+// the FP64 form, the FP32 copies for the mixed form with FP32 copies
+// (primitives, ghosts, face states, boundary fluxes, optional dumps).
+template <typename T>
+struct StageIO;
+template <>
+struct StageIO<double> {
+  static __device__ __forceinline__ const double* vin(const StageArgs& a) { return a.Vin; }
+  static __device__ __forceinline__ const double* vg(const StageArgs& a) { return a.vg; }
+  static __device__ __forceinline__ double* fs(const StageArgs& a) { return a.fs; }
+  static __device__ __forceinline__ const double* fb(const StageArgs& a) { return a.fb; }
+  static __device__ __forceinline__ double* grad(const StageArgs& a) { return a.grad; }
+  static __device__ __forceinline__ double* phi(const StageArgs& a) { return a.phi; }
+};
+template <>
+struct StageIO<float> {
+  static __device__ __forceinline__ const float* vin(const StageArgs& a) { return a.Vin32; }
+  static __device__ __forceinline__ const float* vg(const StageArgs& a) { return a.vg32; }
+  static __device__ __forceinline__ float* fs(const StageArgs& a) { return a.fs32; }
+  static __device__ __forceinline__ const float* fb(const StageArgs& a) { return a.fb32; }
+  static __device__ __forceinline__ float* grad(const StageArgs& a) { return a.grad32; }
+  static __device__ __forceinline__ float* phi(const StageArgs& a) { return a.phi32; }
+};
 
 // device scalars: the step's dt (minimum), the time, t_end, the dt last used,
 // and the next step's dt while the last stage computes it
@@ -580,10 +620,9 @@ template <typename T, int kPipe, bool kDS = false>
 __device__ __forceinline__ void gradient_node_cell(const MeshView<T>& m, const StageArgs& a, int c, T vown[5],
                                                    T* dS_out = nullptr) {
   const int st = m.stride;
-  static_assert(sizeof(T) == 8, "FP64 kernel");
-  const T* __restrict__ Vin = a.Vin;
-  const T* __restrict__ Vg = a.vg;
-  T* __restrict__ fsc = a.fs + c;  // this cell's column of the face states
+  const T* __restrict__ Vin = StageIO<T>::vin(a);
+  const T* __restrict__ Vg = StageIO<T>::vg(a);
+  T* __restrict__ fsc = StageIO<T>::fs(a) + c;  // this cell's column of the face states
   int nb[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) nb[q] = checked_nb(m.nbvf[q * st + c], 0, m.n, m.nb, c, a.status);
@@ -682,10 +721,10 @@ __device__ __forceinline__ void gradient_node_cell(const MeshView<T>& m, const S
     }
 #pragma unroll
     for (int q = 0; q < 4; q++) fsc[size_t(q * 5 + k) * st] = fma(phi, gr[q], vc);
-    if (a.grad) {
+    if (T* gdump = StageIO<T>::grad(a)) {
 #pragma unroll
-      for (int e = 0; e < 3; e++) a.grad[(k * 3 + e) * st + c] = g[e];
-      a.phi[k * st + c] = phi;
+      for (int e = 0; e < 3; e++) gdump[(k * 3 + e) * st + c] = g[e];
+      StageIO<T>::phi(a)[k * st + c] = phi;
     }
   };
   if constexpr (kPipe == 2) {
@@ -715,7 +754,7 @@ __device__ __forceinline__ void gradient_node_cell(const MeshView<T>& m, const S
 // Solver.cpp:250; every thread reaches the block minimum).
 template <typename T, int kPipe, int kMinBlocks, bool kDt = false>
 __global__ void __launch_bounds__(128, kMinBlocks) gradient_node_kernel(MeshView<T> m, StageArgs a, DtFuse dtf) {
-  static_assert(sizeof(T) == 8, "FP64 kernel");
+  static_assert(!kDt || sizeof(T) == 8, "the fused time step is the FP64 form's");
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   pdl_launch_dependents();
   pdl_wait_previous();
@@ -781,13 +820,27 @@ __device__ __forceinline__ void stage_update(const StageArgs& a, int c, int st, 
 #pragma unroll
   for (int k = 0; k < 5; k++) {
     a.Uout[k * st + c] = Unew[k];
-    a.Vout[k * st + c] = Vn[k];
+    if (a.Vout) a.Vout[k * st + c] = Vn[k];
+    if (a.Vout32) a.Vout32[k * st + c] = float(Vn[k]);
     if (a.R) a.R[k * st + c] = R[k];
     finite = finite && isfinite(R[k]) && isfinite(Unew[k]);
   }
   if (a.res_cell) a.res_cell[c] = R[0] * ivol;
   if (!finite) atomicOr(a.status, kErrNonFinite);
   else if (!(Vn[0] > 0.0) || !(Vn[4] > 0.0)) atomicOr(a.status, kErrNonPhysical);
+  if (a.dt_next_min) {
+    // the next step's time step from this result's primitives; the minimum
+    // by one atomicMin on the bit pattern (exact for positive doubles),
+    // skipped when the value is not below the current minimum
+    const double d = (a.freeze && dt == 0.0) ? 0.0 : dt_of_cell_fast(Vn, a.dS[c], a.dS[st + c], a.dS[2 * st + c], vol, a.cfl);
+    if (a.dt_next) a.dt_next[c] = d;
+    if (!(a.freeze && dt == 0.0)) {
+      if (!(d > 0.0) && !isnan(d)) atomicOr(a.status, kErrDt);
+      if (d > 0.0 &&
+          d < __longlong_as_double(static_cast<long long>(*reinterpret_cast<volatile unsigned long long*>(a.dt_next_min))))
+        atomicMin(a.dt_next_min, (unsigned long long)__double_as_longlong(d));
+    }
+  }
 }
 
 // kPipe: 0 one face's loads at a time, 1 the next face's loads in flight
@@ -798,13 +851,16 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   pdl_launch_dependents();
   pdl_wait_previous();
-  if (c >= m.n || frozen_cell(a, c)) return;
+  if (c >= m.n) return;
+  if (frozen_cell(a, c)) {
+    if (a.dt_next_min && a.dt_next) a.dt_next[c] = 0.0;  // a converged case keeps its state
+    return;
+  }
   const int st = m.stride;
   const bool second = a.second_order != 0;
-  static_assert(sizeof(T) == 8, "FP64 kernel");
-  const T* __restrict__ fsb = a.fs;
-  const T* __restrict__ Vin = a.Vin;
-  const T* __restrict__ fb = a.fb;
+  const T* __restrict__ fsb = StageIO<T>::fs(a);
+  const T* __restrict__ Vin = StageIO<T>::vin(a);
+  const T* __restrict__ fb = StageIO<T>::fb(a);
   const int code = m.gcode[c];
   int ns[4];
 #pragma unroll

@@ -131,6 +131,71 @@ void launch_gradient_mixed(const MeshView<float>& m, const StageArgs& a, Launch 
 void launch_flux_mixed(const MeshView<float>& m, const StageArgs& a, Launch l) {
   NF_DELTA_DISPATCH(flux_delta_kernel, m, a, l);
 }
+// The mixed form with FP32 copies: ghost states and boundary fluxes computed
+// in FP64 from the FP32 primitives or face states (boundary faces are a few
+// percent of the faces) and stored in FP32 for the FP32 node kernels.
+__global__ void __launch_bounds__(256) ghost32_kernel(MeshView<double> m, StageArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait_previous();
+  if (b >= m.nb) return;
+  const int c = checked(m.b_cell[b], m.n, a.status), f = checked(m.b_face[b], m.n_faces, a.status);
+  const int F = m.n_faces, st = m.stride;
+  double V[5], G[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) V[k] = double(a.Vin32[k * st + c]);
+  const double nh[3] = {m.nhat[f], m.nhat[F + f], m.nhat[2 * F + f]};
+  ghost_state<double>(m.patches[checked(m.b_patch[b], m.n_patches, a.status)], V, nh, G);
+#pragma unroll
+  for (int k = 0; k < 5; k++) a.vg32[k * m.bstride + b] = float(G[k]);
+}
+
+__global__ void __launch_bounds__(256) boundary_flux32_kernel(MeshView<double> m, StageArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  pdl_launch_dependents();
+  pdl_wait_previous();
+  if (b >= m.nb) return;
+  const int c = checked(m.b_cell[b], m.n, a.status), q = checked(m.b_fs[b], 4, a.status),
+            f = checked(m.b_face[b], m.n_faces, a.status);
+  const int F = m.n_faces, st = m.stride;
+  double VL[5], VR[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) VL[k] = double(a.second_order ? a.fs32[(q * 5 + k) * st + c] : a.Vin32[k * st + c]);
+  const double nh[3] = {m.nhat[f], m.nhat[F + f], m.nhat[2 * F + f]};
+  ghost_state<double>(m.patches[checked(m.b_patch[b], m.n_patches, a.status)], VL, nh, VR);
+  double Fl[5];
+  rusanov_fast<double>(VL, VR, nh, m.area[f], Fl);
+#pragma unroll
+  for (int k = 0; k < 5; k++) a.fb32[k * m.bstride + b] = float(Fl[k]);
+}
+
+// mixed form with FP32 copies: the node kernels in FP32 (no fused time step)
+void launch_gradient_m32(const MeshView<float>& m, const StageArgs& a, Launch l) {
+  const DtFuse d{0.0, nullptr, nullptr};
+  const int b = fast_block(l.block);
+  const int g = grid_for(m.n, b);
+  switch (l.variant) {
+    case 1: launch_pdl(gradient_node_kernel<float, 1, 1, false>, g, b, l.stream, m, a, d); break;
+    case 2: launch_pdl(gradient_node_kernel<float, 0, kCap<float>, false>, g, b, l.stream, m, a, d); break;
+    case 3: launch_pdl(gradient_node_kernel<float, 1, kCap<float>, false>, g, b, l.stream, m, a, d); break;
+    case 4: launch_pdl(gradient_node_kernel<float, 0, kCap2<float>, false>, g, b, l.stream, m, a, d); break;
+    case 5: launch_pdl(gradient_node_kernel<float, 1, kCap2<float>, false>, g, b, l.stream, m, a, d); break;
+    case 6: launch_pdl(gradient_node_kernel<float, 2, 1, false>, g, b, l.stream, m, a, d); break;
+    case 7: launch_pdl(gradient_node_kernel<float, 2, kCap3<float>, false>, g, b, l.stream, m, a, d); break;
+    case 8: launch_pdl(gradient_node_kernel<float, 3, kCap<float>, false>, g, b, l.stream, m, a, d); break;
+    case 9: launch_pdl(gradient_node_kernel<float, 3, kCap2<float>, false>, g, b, l.stream, m, a, d); break;
+    default: launch_pdl(gradient_node_kernel<float, 0, 1, false>, g, b, l.stream, m, a, d); break;
+  }
+}
+void launch_flux_m32(const MeshView<float>& m, const StageArgs& a, Launch l) {
+  NF_NODE_DISPATCH(flux_node_kernel, float, m, a, l);
+}
+void launch_ghost_m32(const MeshView<double>& m, const StageArgs& a, Launch l) {
+  if (m.nb > 0) launch_pdl(ghost32_kernel, grid_for(m.nb, l.block), l.block, l.stream, m, a);
+}
+void launch_bflux_m32(const MeshView<double>& m, const StageArgs& a, Launch l) {
+  if (m.nb > 0) launch_pdl(boundary_flux32_kernel, grid_for(m.nb, l.block), l.block, l.stream, m, a);
+}
 void launch_ghost_fast(const MeshView<double>& m, const StageArgs& a, Launch l) {
   if (m.nb > 0) launch_pdl(ghost_kernel<double, false>, grid_for(m.nb, l.block), l.block, l.stream, m, a);
 }

@@ -209,7 +209,11 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_delta_kernel(MeshView<fl
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   pdl_launch_dependents();
   pdl_wait_previous();
-  if (c >= m.n || frozen_cell(a, c)) return;
+  if (c >= m.n) return;
+  if (frozen_cell(a, c)) {
+    if (a.dt_next_min && a.dt_next) a.dt_next[c] = 0.0;  // a converged case keeps its state
+    return;
+  }
   const int st = m.stride;
   const bool second = a.second_order != 0;
   const double* __restrict__ V = a.Vin;

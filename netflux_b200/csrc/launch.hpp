@@ -36,6 +36,12 @@ void launch_bflux_fast(const MeshView<double>& m, const StageArgs& a, Launch l);
 // stored as FP32 differences to the owner's physical flux
 void launch_bflux_mixed(const MeshView<double>& m, const StageArgs& a, Launch l);
 void launch_prim_fast(int n, int stride, const double* U, double* V, float* V32, Launch l);
+// mixed with FP32 copies: the FP32 node kernels and the boundary kernels that
+// read and write the FP32 copies (kernels_fast.cu)
+void launch_gradient_m32(const MeshView<float>& m, const StageArgs& a, Launch l);
+void launch_flux_m32(const MeshView<float>& m, const StageArgs& a, Launch l);
+void launch_ghost_m32(const MeshView<double>& m, const StageArgs& a, Launch l);
+void launch_bflux_m32(const MeshView<double>& m, const StageArgs& a, Launch l);
 // the fast forms' reciprocal and reciprocal square root, elementwise (self-test)
 void launch_fastmath(const double* x, int n, double* rcp, double* rsq, Launch l);
 

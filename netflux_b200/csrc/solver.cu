@@ -276,6 +276,10 @@ struct nf_solver {
   DevBuf<double> Uold;       // U^n of the next step when set apart from U (nf_set_state_old)
   bool old_pending = false;
   DevBuf<float> fs32, grad32, phi32, fb32;  // mixed: increments, fields, boundary flux differences
+  // mixed with FP32 copies: FP32 primitives of successive stage inputs (the
+  // same double-buffering as V0/V1) and FP32 ghost states; fs32 and fb32
+  // hold its face states and boundary fluxes
+  DevBuf<float> V32a, V32b, vg32;
   DevBuf<unsigned> status;
   DevBuf<long long> chunk_begin, chunk_end, case_cells;
   DevBuf<int> case_chunk0;
@@ -363,6 +367,7 @@ struct nf_solver {
   }
 
   double* Vbuf(int i) { return i ? V1.p : V0.p; }
+  float* V32buf(int i) { return i ? V32b.p : V32a.p; }
   // the conserved state stage s reads (Solver.cpp:103-133: U, then the RK
   // stage W)
   double* stage_input(int s) { return (p.time_scheme == NF_TVD_RK3 && s > 0) ? W.p : U.p; }
@@ -372,9 +377,18 @@ struct nf_solver {
   bool fuse_dt() const {
     return p.precision == NF_PREC_FP64 && p.spatial_order == NF_SECOND_ORDER && !p.dt_from_current_state;
   }
-  void launch_prim(const double* Usrc, double* V) {
-    if (p.precision == NF_PREC_FP64_REF) nf::launch_prim_ref(n, stride, Usrc, V, nullptr, launch());
-    else nf::launch_prim_fast(n, stride, Usrc, V, nullptr, launch());
+  // the mixed forms (TVD-RK3): the stage-2 flux kernel computes the next
+  // step's dt from the primitives of its result, the last stage's input
+  bool fuse_dt_flux() const {
+    return (p.precision == NF_PREC_MIXED || p.precision == NF_PREC_MIXED32) && p.time_scheme == NF_TVD_RK3 &&
+           !p.dt_from_current_state;
+  }
+  // primitives of Usrc into primitive buffer b (and its FP32 copy in the
+  // mixed form with FP32 copies)
+  void launch_prim(const double* Usrc, int b) {
+    float* v32 = p.precision == NF_PREC_MIXED32 ? V32buf(b) : nullptr;
+    if (p.precision == NF_PREC_FP64_REF) nf::launch_prim_ref(n, stride, Usrc, Vbuf(b), nullptr, launch());
+    else nf::launch_prim_fast(n, stride, Usrc, Vbuf(b), v32, launch());
   }
   nf::Launch launch() const { return nf::Launch{block, stream}; }
 
@@ -413,7 +427,7 @@ struct nf_solver {
 
   // primitives of U in both V buffers (as after nf_set_state)
   void refresh_primitives() {
-    for (int b = 0; b < 2; b++) launch_prim(U.p, Vbuf(b));
+    for (int b = 0; b < 2; b++) launch_prim(U.p, b);
   }
 
   void ratchet_reset() {
@@ -491,14 +505,28 @@ struct nf_solver {
   void launch_gradient(const nf::StageArgs& a, const KCfg& k, const nf::DtFuse* dtf = nullptr) {
     const nf::Launch l{k.block, stream, k.variant};
     if (p.precision == NF_PREC_MIXED) nf::launch_gradient_mixed(view32(), a, l);
+    else if (p.precision == NF_PREC_MIXED32) nf::launch_gradient_m32(view32(), a, l);
     else if (p.precision == NF_PREC_FP64) nf::launch_gradient_fast(view64(), a, dtf, l);
     else nf::launch_gradient_ref(view64(), a, launch());
   }
   void launch_flux(const nf::StageArgs& a, const KCfg& k) {
     const nf::Launch l{k.block, stream, k.variant};
     if (p.precision == NF_PREC_MIXED) nf::launch_flux_mixed(view32(), a, l);
+    else if (p.precision == NF_PREC_MIXED32) nf::launch_flux_m32(view32(), a, l);
     else if (p.precision == NF_PREC_FP64) nf::launch_flux_fast(view64(), a, l);
     else nf::launch_flux_ref(view64(), a, launch());
+  }
+  // ghost states and boundary fluxes of the stage, in each form's precision
+  void launch_ghost(const nf::StageArgs& a) {
+    if (p.precision == NF_PREC_FP64_REF) nf::launch_ghost_ref(view64(), a, launch());
+    else if (p.precision == NF_PREC_MIXED32) nf::launch_ghost_m32(view64(), a, launch());
+    else nf::launch_ghost_fast(view64(), a, launch());
+  }
+  void launch_bflux(const nf::StageArgs& a) {
+    if (p.precision == NF_PREC_MIXED) nf::launch_bflux_mixed(view64(), a, launch());
+    else if (p.precision == NF_PREC_MIXED32) nf::launch_bflux_m32(view64(), a, launch());
+    else if (p.precision == NF_PREC_FP64) nf::launch_bflux_fast(view64(), a, launch());
+    else nf::launch_bflux_ref(view64(), a, launch());
   }
   // launch variants the tuner may pick (gradient, flux)
   int grad_variants() const { return 10; }
@@ -519,6 +547,11 @@ struct nf_solver {
     a.vg = vg.p;
     a.fb = fb.p;
     a.fb32 = fb32.p;
+    if (p.precision == NF_PREC_MIXED32) {
+      a.Vin32 = V32buf(vcur);
+      a.Vout32 = V32buf(1 - vcur);
+      a.vg32 = vg32.p;
+    }
     a.dt_local = dtl(dtl_cur);
     a.scal = scal.p;
     a.status = status.p;
@@ -535,8 +568,13 @@ struct nf_solver {
     if (p.precision == NF_PREC_FP64_REF) return;  // reference form: fixed shape
     const int other = 1 - vcur;
     std::vector<double> keep(size_t(5) * stride);
+    std::vector<float> keep32(p.precision == NF_PREC_MIXED32 ? size_t(5) * stride : 0);
     ck(cudaMemcpyAsync(keep.data(), Vbuf(other), keep.size() * sizeof(double), cudaMemcpyDeviceToHost, stream),
        "tune save");
+    if (!keep32.empty())
+      ck(cudaMemcpyAsync(keep32.data(), V32buf(other), keep32.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                         stream),
+         "tune save");
     ck(cudaStreamSynchronize(stream), "tune sync");
     nf::StageArgs a = first_stage_args();
     cudaEvent_t e0, e1;
@@ -559,7 +597,7 @@ struct nf_solver {
       return c;
     };
     if (a.second_order) {
-      nf::launch_ghost_fast(view64(), a, launch());
+      launch_ghost(a);
       float best = 1e30f;
       for (const KCfg& k : cands(grad_variants())) {
         const float t = time_it([&] { launch_gradient(a, k); });
@@ -570,8 +608,7 @@ struct nf_solver {
       }
       launch_gradient(a, kgrad);
     }
-    if (p.precision == NF_PREC_MIXED) nf::launch_bflux_mixed(view64(), a, launch());
-    else nf::launch_bflux_fast(view64(), a, launch());
+    launch_bflux(a);
     float best = 1e30f;
     for (const KCfg& k : cands(flux_variants())) {
       const float t = time_it([&] { launch_flux(a, k); });
@@ -584,6 +621,10 @@ struct nf_solver {
     cudaEventDestroy(e1);
     ck(cudaMemcpyAsync(Vbuf(other), keep.data(), keep.size() * sizeof(double), cudaMemcpyHostToDevice, stream),
        "tune restore");
+    if (!keep32.empty())
+      ck(cudaMemcpyAsync(V32buf(other), keep32.data(), keep32.size() * sizeof(float), cudaMemcpyHostToDevice,
+                         stream),
+         "tune restore");
     ck(cudaMemsetAsync(status.p, 0, sizeof(unsigned), stream), "status reset");
     ck(cudaStreamSynchronize(stream), "tune sync");
     for (auto& g : graph)
@@ -604,7 +645,7 @@ struct nf_solver {
   // One stage of the step; the last one also ends the step.
   void enqueue_stage(int s) {
     const int n_stages = this->n_stages();
-    const bool fuse = fuse_dt();
+    const bool fuse = fuse_dt() || fuse_dt_flux();
     nf::DtFuse dtf{p.cfl, p.local_time_stepping ? dtl(1 - dtl_cur) : nullptr,
                    reinterpret_cast<unsigned long long*>(scal.p + nf::kScalDtNext)};
     {
@@ -650,24 +691,38 @@ struct nf_solver {
         a.Un = old_pending ? Uold.p : U.p;
         a.Uout = U.p;
       }
-      if (p.precision == NF_PREC_MIXED) {
+      if (p.precision == NF_PREC_MIXED32) {
+        a.Vin32 = V32buf(vcur);
+        a.Vout32 = V32buf(1 - vcur);
+        a.vg32 = vg32.p;
+        // the FP64 primitives only where a time-step kernel reads them: the
+        // state the next time step reads (the last stage's input, Q3, or with
+        // dt_from_current_state the step's result), unless the stage-2 flux
+        // kernel computes that time step itself from its FP64 result
+        const int dt_stage = p.dt_from_current_state ? n_stages - 1 : std::max(n_stages - 2, 0);
+        if (s != dt_stage || fuse_dt_flux()) a.Vout = nullptr;
+      }
+      if (fuse_dt_flux() && s == n_stages - 2) {
+        a.dt_next = dtf.dt_next;
+        a.dt_next_min = dtf.dt_min_bits;
+        a.dS = dS.p;
+        a.cfl = p.cfl;
+      }
+      if (p.precision == NF_PREC_MIXED || p.precision == NF_PREC_MIXED32) {
         a.fs32 = fs32.p;
         a.grad32 = p.keep_stage_fields ? grad32.p : nullptr;
         a.phi32 = p.keep_stage_fields ? phi32.p : nullptr;
       }
       if (a.second_order) {
         prof_begin(NF_KERNEL_OTHER);
-        if (p.precision == NF_PREC_FP64_REF) nf::launch_ghost_ref(view64(), a, launch());
-        else nf::launch_ghost_fast(view64(), a, launch());
+        launch_ghost(a);
         prof_end();
         prof_begin(NF_KERNEL_GRADIENT);
-        launch_gradient(a, kgrad, (fuse && s == n_stages - 1) ? &dtf : nullptr);
+        launch_gradient(a, kgrad, (fuse_dt() && s == n_stages - 1) ? &dtf : nullptr);
         prof_end();
       }
       prof_begin(NF_KERNEL_OTHER);
-      if (p.precision == NF_PREC_MIXED) nf::launch_bflux_mixed(view64(), a, launch());
-      else if (p.precision == NF_PREC_FP64) nf::launch_bflux_fast(view64(), a, launch());
-      else nf::launch_bflux_ref(view64(), a, launch());
+      launch_bflux(a);
       prof_end();
       prof_begin(NF_KERNEL_FLUX);
       launch_flux(a, kflux);
@@ -717,7 +772,7 @@ struct nf_solver {
   void adopt_state(const double* aos) {
     const int st = stride;
     scatter_state_kernel<<<(n + 255) / 256, 256, 0, stream>>>(n, st, d_dev_of_ref.p, aos, U.p);
-    for (int b = 0; b < 2; b++) launch_prim(U.p, Vbuf(b));
+    for (int b = 0; b < 2; b++) launch_prim(U.p, b);
     vcur = 0;
     dtl_cur = 0;
     dt_ready = false;
@@ -1052,7 +1107,7 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     if (p.limiter != NF_LIMITER_NONE && p.limiter != NF_LIMITER_BARTH) throw std::runtime_error("bad limiter");
     if (p.flux_scheme != NF_FLUX_RUSANOV)
       throw std::runtime_error("only the Rusanov flux is implemented (the reference's HLLC is a stub)");
-    if (p.precision < NF_PREC_FP64_REF || p.precision > NF_PREC_MIXED) throw std::runtime_error("bad precision");
+    if (p.precision < NF_PREC_FP64_REF || p.precision > NF_PREC_MIXED32) throw std::runtime_error("bad precision");
     if (p.patches && p.n_patches != int(m.patches.size()))
       throw std::runtime_error("params.n_patches does not match the mesh's patch count");
     s->p = p;
@@ -1269,7 +1324,7 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
       for (int64_t v = 0; v < m.n_nodes; v++)
         for (int e = 0; e < 3; e++) n4[size_t(4 * v + e)] = m.nodes[size_t(3 * v + e)];
       s->nodes4.upload(n4, st);
-      if (p.precision == NF_PREC_MIXED) {
+      if (p.precision == NF_PREC_MIXED || p.precision == NF_PREC_MIXED32) {
         std::vector<float> n4f(n4.size());
         for (size_t i = 0; i < n4.size(); i++) n4f[i] = float(n4[i]);
         s->nodes4_32.upload(n4f, st);
@@ -1281,7 +1336,14 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     s->vol.upload(h_vol, st);
     s->dS.upload(h_dS, st);
     s->patches.upload(h_pb, st);
-    if (p.precision == NF_PREC_MIXED) {
+    const bool fp32_fields = p.precision == NF_PREC_MIXED || p.precision == NF_PREC_MIXED32;
+    if (p.precision == NF_PREC_MIXED32) {
+      s->V32a.alloc(size_t(5) * stride);
+      s->V32b.alloc(size_t(5) * stride);
+      s->vg32.alloc(size_t(5) * s->bstride);
+      s->vg32.zero(st);
+    }
+    if (fp32_fields) {
       s->fb32.alloc(size_t(5) * s->bstride);
       s->fb32.zero(st);
       s->fs32.alloc(size_t(20) * stride);
@@ -1299,7 +1361,7 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     s->V1.alloc(size_t(5) * stride);
     s->vg.alloc(size_t(5) * s->bstride);  // FP64 ghosts in every form
     s->vg.zero(st);
-    if (p.precision != NF_PREC_MIXED) {
+    if (!fp32_fields) {
       s->fs.alloc(size_t(20) * stride);
       s->fs.zero(st);
       s->fb.alloc(size_t(5) * s->bstride);
@@ -1308,7 +1370,7 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
     if (p.keep_stage_fields) {
       s->R.alloc(size_t(5) * stride);
       s->R.zero(st);
-      if (p.precision != NF_PREC_MIXED) {
+      if (!fp32_fields) {
         s->grad.alloc(size_t(15) * stride);
         s->phi.alloc(size_t(5) * stride);
         s->grad.zero(st);
@@ -1360,7 +1422,7 @@ nf_solver* nf_create(const nf_mesh* h, const nf_params* params) {
       s->ratchet_alloc = true;
       s->case_ratchet.alloc(size_t(s->n_cases));
       s->h_ratchet.assign(size_t(s->n_cases), 0);
-      if (p.precision == NF_PREC_MIXED) s->phi_keep32.alloc(size_t(5) * stride);
+      if (p.precision == NF_PREC_MIXED || p.precision == NF_PREC_MIXED32) s->phi_keep32.alloc(size_t(5) * stride);
       else s->phi_keep.alloc(size_t(5) * stride);
       s->ratchet_reset();
     }
@@ -1608,6 +1670,10 @@ static int halo_args(nf_solver* s, const int64_t* cells, int64_t n, const double
     s->err = std::string(what) + ": null pointer or negative count";
     return NF_ERR_ARG;
   }
+  if (s->p.precision == NF_PREC_MIXED32) {
+    s->err = std::string(what) + ": the mixed form with FP32 copies keeps its stage primitives in FP32 only";
+    return NF_ERR_UNSUPPORTED;
+  }
   return NF_OK;
 }
 
@@ -1826,13 +1892,17 @@ int nf_get_field(nf_solver* s, int which, double* out, int64_t n_values) {
       return NF_ERR_ARG;
     }
     std::vector<double> h(size_t(comps) * st);
-    if (s->p.precision == NF_PREC_MIXED && (which == NF_FIELD_GRADIENT || which == NF_FIELD_LIMITER)) {
-      if (!s->grad32.p) {
+    const bool m32_prim = s->p.precision == NF_PREC_MIXED32 && which == NF_FIELD_PRIMVARS && s->stepped;
+    if (((s->p.precision == NF_PREC_MIXED || s->p.precision == NF_PREC_MIXED32) &&
+         (which == NF_FIELD_GRADIENT || which == NF_FIELD_LIMITER)) ||
+        m32_prim) {
+      if (!m32_prim && !s->grad32.p) {
         s->err = "nf_get_field: field not kept (set keep_stage_fields)";
         return NF_ERR_ARG;
       }
+      // the mixed form with FP32 copies keeps the stage primitives in FP32
       std::vector<float> hf(size_t(comps) * st);
-      const float* src32 = which == NF_FIELD_GRADIENT ? s->grad32.p : s->phi32.p;
+      const float* src32 = m32_prim ? s->V32buf(1 - s->vcur) : which == NF_FIELD_GRADIENT ? s->grad32.p : s->phi32.p;
       ck(cudaMemcpyAsync(hf.data(), src32, hf.size() * sizeof(float), cudaMemcpyDeviceToHost, s->stream), "D2H");
       ck(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
       for (size_t i = 0; i < hf.size(); i++) h[i] = hf[i];
@@ -2020,6 +2090,9 @@ nf_split* nf_split_create(nf_solver* const* parts, int n_parts) {
           s->p.dt_from_current_state != p0.dt_from_current_state)
         throw std::invalid_argument("nf_split_create: the parts' solver parameters differ");
       if (s->stage_next != 0) throw std::invalid_argument("nf_split_create: a part is inside a step");
+      if (s->p.precision == NF_PREC_MIXED32)
+        throw std::invalid_argument("nf_split_create: the mixed form with FP32 copies is not split (its halo would "
+                                    "need the FP32 primitives exchanged)");
       for (int j = 0; j < i; j++)
         if (parts[j] == s) throw std::invalid_argument("nf_split_create: a part is listed twice");
       sp->parts.push_back(s);

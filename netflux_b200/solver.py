@@ -31,10 +31,11 @@ BOUNDARY_TYPES = {"NoSlipWall": L.NF_BC_NO_SLIP_WALL, "SlipWall": L.NF_BC_SLIP_W
 TIME_SCHEMES = {"ExplicitEuler": L.NF_EXPLICIT_EULER, "TVD_RK3": L.NF_TVD_RK3}
 SPATIAL_ORDERS = {"First": L.NF_FIRST_ORDER, "Second": L.NF_SECOND_ORDER}
 LIMITERS = {"NONE": L.NF_LIMITER_NONE, "Barth": L.NF_LIMITER_BARTH}
-PRECISIONS = {"fp64_ref": L.NF_PREC_FP64_REF, "fp64": L.NF_PREC_FP64, "mixed": L.NF_PREC_MIXED}
+PRECISIONS = {"fp64_ref": L.NF_PREC_FP64_REF, "fp64": L.NF_PREC_FP64, "mixed": L.NF_PREC_MIXED,
+              "mixed32": L.NF_PREC_MIXED32}
 STANDARD_AIR = (1.225, 0.0, 0.0, 0.0, 101325.0)  # Utilities.hpp:100-107
 # launch variants of the gradient and flux kernels each arithmetic form offers (the tuner's candidates)
-LAUNCH_VARIANTS = {"fp64_ref": (10, 10), "fp64": (10, 10), "mixed": (10, 10)}
+LAUNCH_VARIANTS = {"fp64_ref": (10, 10), "fp64": (10, 10), "mixed": (10, 10), "mixed32": (10, 10)}
 
 
 def _check(rc: int, handle=None) -> None:

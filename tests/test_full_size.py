@@ -177,13 +177,14 @@ def test_config3_bump_3m_cells_one_step_against_oracle():
     for label, U0 in starts.items():
         oracle = Background(po.run_oracle, grid, pats, [fs] * len(pats), U0, 1, local_time_stepping=True,
                             fields=False)
-        out = {p: _gpu(mesh, U0, p, 1, fs, local_time_stepping=True) for p in ("fp64", "mixed")}
+        out = {p: _gpu(mesh, U0, p, 1, fs, local_time_stepping=True) for p in ("fp64", "mixed", "mixed32")}
         o = oracle.result()["U"]
         _report(f"config 3 ({label}), 1 step vs oracle,", {p: (U, o) for p, U in out.items()})
         print("  max change of the step", rel_linf(o, U0))
         assert rel_linf(o, U0) > 1e-8  # the step changed the state
         assert rel_linf(out["fp64"], o) <= TOL_FP64_1, label
         assert rel_linf(out["mixed"], o) <= TOL_MIXED_1, label
+        assert rel_linf(out["mixed32"], o) <= TOL_MIXED_1, label
 
 
 @pytest.mark.skipif(os.environ.get("NETFLUX_LONG_PARITY") != "1",

@@ -89,13 +89,24 @@ def test_ref_order_hundred_steps(case):
     assert rel_linf(U, g["U100"]) <= 1e-12
 
 
+@pytest.mark.parametrize("precision", ["mixed", "mixed32"])
 @pytest.mark.parametrize("case", CASES)
-def test_mixed_one_step(case):
+def test_mixed_one_step(case, precision):
     g = golden(case)
-    _, U, _ = run(g, "mixed", 1)
-    print(case, "mixed one step: Linf", rel_linf(U, g["U1"]), "L2", rel_l2(U, g["U1"]))
+    _, U, _ = run(g, precision, 1)
+    print(case, precision, "one step: Linf", rel_linf(U, g["U1"]), "L2", rel_l2(U, g["U1"]))
     err = rel_linf(U, g["U1"])
     assert err <= TOL_MIXED_1, err
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_mixed32_hundred_steps(case):
+    """The mixed form with FP32 copies over 100 steps of the compiled reference's run: its error
+    grows with the FP32 rounding of the primitives it gathers (stated, bounded loosely)."""
+    g = golden(case)
+    _, U, _ = run(g, "mixed32", 100, use_advance=True)
+    print(case, "mixed32 100 steps: Linf", rel_linf(U, g["U100"]), "L2", rel_l2(U, g["U100"]))
+    assert rel_linf(U, g["U100"]) <= 1e-3
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -113,7 +124,7 @@ def test_advance_graph_equals_step_loop():
     assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed32"])
 def test_tuning_changes_nothing(precision):
     """Tuned launch shapes compute the same bits and leave the state untouched."""
     g = golden("bump12")
@@ -130,7 +141,7 @@ def test_tuning_changes_nothing(precision):
     assert np.array_equal(a.get_solver_data().get_solution(), b.get_solver_data().get_solution())
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed32"])
 def test_every_launch_variant_computes_the_same_bits(precision):
     """Every block size and variant the tuner may pick (pipelined loads, register caps) gives the same state."""
     g = golden("bump12")
@@ -175,17 +186,20 @@ def _oracle(g, n, **kw):
     return po.run_oracle(m.export(), pats, [g["freestream"]] * len(pats), g["U0"], n, **kw)
 
 
-def test_fused_time_step_matches_oracle():
-    """FP64: from the second step on, the time step comes from the last stage's gradient kernel
-    (the last stage input's primitives, projected areas from the normals in registers, the fast
-    reciprocals); each step's dt agrees with the oracle's calc_timestep to a few ulp."""
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-14), ("mixed", 1e-6), ("mixed32", 1e-5)])
+def test_fused_time_step_matches_oracle(precision, tol):
+    """From the second step on the time step is computed inside the step: FP64 by the last stage's
+    gradient kernel (the last stage input's primitives, projected areas from the normals in
+    registers), the mixed forms by the stage-2 flux kernel from the FP64 primitives of its result
+    (the same state). Each step's dt agrees with the oracle's calc_timestep: FP64 to a few ulp, the
+    mixed forms to their state's own error."""
     g = golden("bump12")
-    _, U, dts = run(g, "fp64", 20)
+    _, U, dts = run(g, precision, 20)
     o = _oracle(g, 20, fields=False)
     err = np.abs(dts - o["dt"]) / o["dt"]
-    print("fused dt vs oracle: max rel", err.max())
-    assert err.max() <= 1e-14
-    assert rel_linf(U, o["U"]) <= 1e-12
+    print(precision, "fused dt vs oracle: max rel", err.max())
+    assert err.max() <= tol
+    assert rel_linf(U, o["U"]) <= (1e-12 if precision == "fp64" else 1e-4)
 
 
 def test_local_time_stepping_matches_oracle():
@@ -416,6 +430,26 @@ def test_steady_mixed_lands_on_the_fp64_state():
         res[prec] = s.get_solver_data().get_solution()
     print("steady mixed vs fp64: L2", rel_l2(res["mixed"], res["fp64"]), "Linf", rel_linf(res["mixed"], res["fp64"]))
     assert rel_l2(res["mixed"], res["fp64"]) <= 1e-5
+
+
+def test_steady_residual_of_the_two_mixed_forms():
+    """The difference form reaches a 1e-6 density-residual drop like FP64; the form with FP32 copies
+    of the primitives rounds every gathered value at |V| 2^-24, and its residual stalls above that
+    (the reached drop is printed; it must still fall by three decades)."""
+    m, fs = _bump_case(12, 0.1, 0.5)
+    mm = S.Mesh.from_tet_mesh(m)
+    U0 = mg.uniform_state(mm.n_cells, fs)
+    out = {}
+    for prec in ("mixed", "mixed32"):
+        cfg = config_for(precision=prec, limiter="NONE", local_time_stepping=True, freestream=fs)
+        s = S.EulerSolver(cfg, mm, U0=U0)
+        out[prec] = s.solve_steady(tol=1e-6, max_steps=20000, check_every=25)
+        s.close()
+        r = out[prec]
+        print(prec, "steady: converged", bool(r["converged"][0]), "steps", int(r["steps"][0]),
+              "drop", float(r["res"][0] / r["res0"][0]))
+    assert out["mixed"]["converged"][0]
+    assert out["mixed32"]["res"][0] <= 1e-3 * out["mixed32"]["res0"][0]
 
 
 def test_batched_steady_freezes_converged_cases_exactly():
