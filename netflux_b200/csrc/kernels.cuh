@@ -626,11 +626,20 @@ __device__ __forceinline__ void gradient_node_cell(const MeshView<T>& m, const S
   int nb[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) nb[q] = checked_nb(m.nbvf[q * st + c], 0, m.n, m.nb, c, a.status);
-  auto fetch = [&](int k, T& vc, T vo[4]) {
-    const T* Vk = Vin + k * st;
-    vc = Vk[c];
+  // each face's row base and row stride (a cell's or a ghost's) chosen once,
+  // so a variable's neighbour load is one address computation
+  const T* qb[4];
+  int qs[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) vo[q] = nb[q] >= 0 ? Vk[nb[q]] : Vg[k * m.bstride + (-nb[q] - 1)];
+  for (int q = 0; q < 4; q++) {
+    const bool cell = nb[q] >= 0;
+    qb[q] = cell ? Vin + nb[q] : Vg + (-nb[q] - 1);
+    qs[q] = cell ? st : m.bstride;
+  }
+  auto fetch = [&](int k, T& vc, T vo[4]) {
+    vc = Vin[size_t(k) * st + c];
+#pragma unroll
+    for (int q = 0; q < 4; q++) vo[q] = qb[q][k * qs[q]];
   };
   if constexpr (kPipe == 3) {
 #pragma unroll
@@ -639,8 +648,7 @@ __device__ __forceinline__ void gradient_node_cell(const MeshView<T>& m, const S
   [[maybe_unused]] T vcN, voN[4];
   [[maybe_unused]] T vcA[5], voA[5][4];
   if constexpr (kPipe == 2) {
-    // the same loads as fetch(), with each face's row base and row stride
-    // chosen once (cell row or ghost row) instead of per variable
+    // the same loads as fetch(), all five variables' at once
 #pragma unroll
     for (int k = 0; k < 5; k++) vcA[k] = Vin[size_t(k) * st + c];
 #pragma unroll

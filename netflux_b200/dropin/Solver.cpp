@@ -24,7 +24,7 @@
 //                                           Output.cpp:19-21) or at the last one
 //   evaluate_* / set_constant_ghost_values  done by the device step
 //
-// Environment: NETFLUX_B200_PRECISION = fp64 (default) | fp64_ref | mixed.
+// Environment: NETFLUX_B200_PRECISION = fp64 (default) | fp64_ref | mixed | mixed32.
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -83,6 +83,7 @@ int precision_from_env() {
   if (!v || !*v || std::strcmp(v, "fp64") == 0) return NF_PREC_FP64;
   if (std::strcmp(v, "fp64_ref") == 0) return NF_PREC_FP64_REF;
   if (std::strcmp(v, "mixed") == 0) return NF_PREC_MIXED;
+  if (std::strcmp(v, "mixed32") == 0) return NF_PREC_MIXED32;
   throw std::runtime_error(std::string("NETFLUX_B200_PRECISION: unknown value ") + v);
 }
 
