@@ -28,6 +28,8 @@
 // four threads per cell (one per face slot).
 #pragma once
 
+#include <type_traits>
+
 #include <cuda_runtime.h>
 
 #include "euler.cuh"
@@ -913,7 +915,10 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
     load_vertices(m, c, P, a.status);
     face_normals(P, S);
   }
-  double R[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  // the flux balance in FP64 (FP64 form); the FP32 form sums its FP32 fluxes
+  // in FP32 and hands the sum to the FP64 update
+  using Acc = typename std::conditional<sizeof(T) == 8, double, float>::type;
+  Acc R[5] = {Acc(0), Acc(0), Acc(0), Acc(0), Acc(0)};
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     FaceIn<T> cur;
@@ -927,7 +932,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
     }
     if (cur.kind == 3) {
 #pragma unroll
-      for (int k = 0; k < 5; k++) R[k] -= double(cur.s[k]);
+      for (int k = 0; k < 5; k++) R[k] -= Acc(cur.s[k]);
     } else if (cur.kind != 0) {
       const int bits = code >> (3 * q);
       const bool own = cur.kind == 1;
@@ -942,10 +947,11 @@ __global__ void __launch_bounds__(128, kMinBlocks) flux_node_kernel(MeshView<T> 
       if (own) rusanov_fast<T>(cur.s, cur.x, nh, area, Fl);
       else rusanov_fast<T>(cur.x, cur.s, nh, area, Fl);
 #pragma unroll
-      for (int k = 0; k < 5; k++) R[k] = own ? R[k] - double(Fl[k]) : R[k] + double(Fl[k]);
+      for (int k = 0; k < 5; k++) R[k] = own ? R[k] - Acc(Fl[k]) : R[k] + Acc(Fl[k]);
     }
   }
-  stage_update(a, c, st, R, m.vol[c]);
+  const double Rd[5] = {double(R[0]), double(R[1]), double(R[2]), double(R[3]), double(R[4])};
+  stage_update(a, c, st, Rd, m.vol[c]);
 }
 
 // ---------------------------------------------------------------------------
