@@ -209,6 +209,8 @@ def main(argv=None):
                     help="none: the unlimited scheme; barth-ratchet: the reference's Barth limiter, ratcheted "
                          "once a case's residual has dropped 1e-2 (needed where the flow turns transonic)")
     ap.add_argument("--eval-check-every", type=int, default=100)
+    ap.add_argument("--eval-skip", type=int, default=0,
+                    help="leave out the first pairs of the held-out list (evaluated in an earlier run)")
     ap.add_argument("--load-mlp", default="", help="start from these parameters (.npy) instead of training")
     ap.add_argument("--skip-sweep", action="store_true", help="with --load-mlp: no sweep, no training")
     ap.add_argument("--out", required=True)
@@ -293,6 +295,7 @@ def finish(a, summary: Dict, mlp: sur.MLP, world: int):
     """Warm-start evaluation on held-out pairs, the optional headline, the summary file."""
     rng = np.random.default_rng(a.seed + 1)
     pairs = [{"mach": float(rng.uniform(*a.mach)), "h": float(rng.uniform(*a.h))} for _ in range(a.eval_pairs)]
+    pairs = pairs[a.eval_skip:]
     rows = evaluate(mlp, pairs, a.eval_nx, a.precision, a.tol, a.max_steps, a.limiter, a.eval_check_every)
     summary["eval"] = rows
     ok = [r for r in rows if r["time_ratio"] is not None]
