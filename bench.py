@@ -183,22 +183,25 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
         (80); per node 16; per boundary face an FP64 ghost (40).
       flux: own V (40), own increments (80), neighbour face ids (16), code (4),
         vertex ids (16), U, U^n, vol, dt, writes U, V and R_rho as above; per
-        node 16; per boundary face an FP32 flux difference (20).
+        node 16; per boundary face an FP32 flux difference (20); stage 2 also
+        reads dS (24) and writes the next step's dt (8 with local time
+        stepping): a third of that on average.
     Mixed with FP32 copies (the FP32 node kernels, NF_PREC_MIXED32):
       gradient: FP32 V (20), ids (32), code (4), vol (8), writes 4 FP32 face
         states (80); per node 16; per boundary face an FP32 ghost (20).
       flux: 4 own FP32 face states (80), neighbour face ids (16), code (4),
-        vertex ids (16), U, U^n, vol, dt, writes U (40), the FP32 V (20), the
-        FP64 V of the state the next time step reads (40 once a step: 1/3 on
-        average) and R_rho; per node 16; per boundary face an FP32 flux (20).
+        vertex ids (16), U, U^n, vol, dt, writes U (40), the FP32 V (20) and
+        R_rho (no FP64 V: the stage-2 flux kernel computes the next dt from its
+        FP64 result); per node 16; per boundary face an FP32 flux (20); the
+        next step's dt as in the difference form.
     """
     lts = 8 if local_dt else 0
     upd = 40 + 40 * 2 / 3 + 8 + lts + 80 + 8 / 3  # U, U^n, vol, dt, U and V out, R_rho
     if precision == "mixed":
         grad = n_cells * (40 + 16 + 16 + 4 + 8 + 80) + n_nodes * 16 + n_boundary * 40
-        flux = n_cells * (40 + 80 + 16 + 4 + 16 + upd) + n_nodes * 16 + n_boundary * 20
+        flux = n_cells * (40 + 80 + 16 + 4 + 16 + upd + (24 + lts) / 3) + n_nodes * 16 + n_boundary * 20
     elif precision == "mixed32":
-        upd32 = 40 + 40 * 2 / 3 + 8 + lts + 40 + 20 + 40 / 3 + 8 / 3
+        upd32 = 40 + 40 * 2 / 3 + 8 + lts + 40 + 20 + 8 / 3 + (24 + lts) / 3
         grad = n_cells * (20 + 16 + 16 + 4 + 8 + 80) + n_nodes * 16 + n_boundary * 20
         flux = n_cells * (80 + 16 + 4 + 16 + upd32) + n_nodes * 16 + n_boundary * 20
     else:
@@ -211,11 +214,11 @@ def algorithmic_bytes(n_cells: int, n_faces: int, n_boundary: int, n_nodes: int,
 # with ncu on the full 3,145,728-tet bump channel with the tuned launch shapes, averaged over the
 # three stages of a step like the event-timed launch durations (FP64: gradient 64/7, flux 64/9,
 # stages 755.3 / 749.8 / 780.6 and 1108.6 / 1221.7 / 1227.9 MB; mixed: gradient 64/7, flux
-# 128/8, stages 503.3 / 501.1 / 500.4 and 978.2 / 1095.4 / 1090.5 MB); the bump workload's
+# 128/8, stages 506.9 / 500.9 / 500.7 and 989.5 / 1208.8 / 1104.6 MB); the bump workload's
 # `roofline.traffic` is this times its cells, other workloads report null.
 MEASURED_DRAM_BYTES_PER_CELL = {
     ("fp64", "gradient"): 761.9e6 / 3145728, ("fp64", "flux"): 1186.1e6 / 3145728,
-    ("mixed", "gradient"): 501.6e6 / 3145728, ("mixed", "flux"): 1054.7e6 / 3145728,
+    ("mixed", "gradient"): 502.8e6 / 3145728, ("mixed", "flux"): 1101.0e6 / 3145728,
 }
 
 

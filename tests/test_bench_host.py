@@ -14,7 +14,7 @@ def test_algorithmic_bytes_per_launch():
     fp64 = bench.algorithmic_bytes(N, F, NB, NODES, "fp64", True)
     mixed = bench.algorithmic_bytes(N, F, NB, NODES, "mixed", True)
     assert round(fp64["gradient"] / 1e6, 1) == 796.7 and round(fp64["flux"] / 1e6, 1) == 1157.4
-    assert round(mixed["gradient"] / 1e6, 1) == 527.9 and round(mixed["flux"] / 1e6, 1) == 1021.2
+    assert round(mixed["gradient"] / 1e6, 1) == 527.9 and round(mixed["flux"] / 1e6, 1) == 1054.7
 
 
 def test_measured_traffic_is_close_to_the_algorithmic_bytes():

@@ -99,6 +99,20 @@ def test_mixed_one_step(case, precision):
     assert err <= TOL_MIXED_1, err
 
 
+@pytest.mark.parametrize("precision", ["mixed", "mixed32"])
+@pytest.mark.parametrize("case", CASES)
+def test_mixed_forms_explicit_euler_and_first_order(case, precision):
+    """The mixed forms on the other schemes: one explicit-Euler step (the time step from the
+    timestep kernel every step) and three first-order steps, against the compiled reference."""
+    g = golden(case)
+    _, U, _ = run(g, precision, 1, time_scheme="ExplicitEuler")
+    e1 = rel_linf(U, g["euler_U"])
+    _, U, _ = run(g, precision, 3, spatial_order="First", limiter="NONE")
+    e3 = rel_linf(U, g["first_U3"])
+    print(case, precision, "explicit Euler 1 step:", e1, "first order 3 steps:", e3)
+    assert e1 <= TOL_MIXED_1 and e3 <= TOL_MIXED_1
+
+
 @pytest.mark.parametrize("case", CASES)
 def test_mixed32_hundred_steps(case):
     """The mixed form with FP32 copies over 100 steps of the compiled reference's run: its error
