@@ -57,6 +57,8 @@ def parse():
                          "drop (minutes)")
     ap.add_argument("--no-steady-quick", action="store_true",
                     help="skip the quick time-to-solution study on a 24x12x12 channel")
+    ap.add_argument("--no-mixed-forms", action="store_true",
+                    help="skip timing the two mixed forms beside the FP64 step (FP64 runs only)")
     ap.add_argument("--steady-max", type=int, default=60000)
     ap.add_argument("--steady-limiter", choices=["none", "barth-ratchet"], default="none")
     ap.add_argument("--block", type=int, default=0, help="fix the block size (no tuning)")
@@ -358,6 +360,33 @@ def host_link(nbytes: int, reps: int = 5):
             "both_total_gbs": round(2 * reps * nbytes / t_both / 1e9, 2)}
 
 
+def mixed_forms(mesh, cfg_kw: dict, U0, steps: int, warmup: int, fp64_ms: float, device: int) -> dict:
+    """The two mixed forms on the benched mesh and state, each tuned and timed like the FP64 step
+    (CUDA events around `steps` graph-replayed steps), with each step's time against the FP64 one
+    measured in the same run: the mixed-precision speed-up the FP64 line is compared with."""
+    from netflux_b200 import _lib as L
+    from netflux_b200 import solver as S
+    lib = L.load()
+    out = {}
+    for prec in ("mixed", "mixed32"):
+        cfg = S.Config(precision=prec, **cfg_kw)
+        s = S.EulerSolver(cfg, mesh, U0=U0, device=device)
+        s.advance(max(warmup, 3) - 2)
+        shapes = s.tune()
+        s.advance(2)
+        ms = C.c_double()
+        kms = (C.c_double * L.NF_KERNEL_COUNT)()
+        kl = (C.c_int64 * L.NF_KERNEL_COUNT)()
+        rc = lib.nf_time_steps(s._h, steps, 0, C.byref(ms), kms, kl)
+        if rc != 0:
+            raise RuntimeError(L.last_error(s._h))
+        s.close()
+        step_ms = ms.value / steps
+        out[prec] = {"value": round(mesh.n_cells * 3 / (step_ms * 1e-3) / 1e6, 3), "ms_per_step": round(step_ms, 5),
+                     "speedup_vs_fp64": round(fp64_ms / step_ms, 4), "launch_shapes": shapes}
+    return out
+
+
 def steady_quick(device: int):
     """Time to a 1e-6 density-residual drop on a small channel (24 x 12 x 12 hexes, 20,736 tets,
     Mach 0.5, h = 0.1, unlimited scheme, local time stepping at CFL 0.8), measured in this run:
@@ -562,6 +591,11 @@ def main():
                   "res_final": float(out["res"][0]),
                   "drop": float(out["res"][0] / out["res0"][0]) if out["res0"][0] > 0 else None}
 
+    mixed = None
+    if rank == 0 and world == 1 and args.precision == "fp64" and not args.no_mixed_forms:
+        mixed = mixed_forms(mesh, dict(CFL=0.8, local_time_stepping=lts, density_fs=fs[0], velocity_fs=list(fs[1:4]),
+                                       pressure_fs=fs[4]), U0, args.steps, args.warmup, dev_ms / args.steps, local)
+
     quick = None
     if rank == 0 and world == 1 and not args.no_steady_quick:
         quick = steady_quick(local)
@@ -596,6 +630,8 @@ def main():
             "gpu_launches": int(round(kernels_per_step * args.steps)),
             "cpu_baseline": cpu,
         }
+        if mixed is not None:
+            line["mixed_forms"] = mixed
         if quick is not None:
             line["steady_quick"] = quick
         if steady is not None:
